@@ -1,0 +1,168 @@
+/* sbh_b200.h - C ABI of the B200-native Stochastic Barnes-Hut summation library.
+ *
+ * libsbh_b200.so replaces the reference's GPU plugin (abhimadan/stochastic-barnes-hut,
+ * src/sbh_gpu.cu) and the host tree containers it consumes (include/py_tree.h,
+ * include/py_tree_gpu.h).  Every entry point is plain C: pointers, sizes and status
+ * codes, no C++ or CUDA types in the signatures (a CUDA stream travels as void*).
+ * The pybind11 modules `sbh` and `sbh_gpu` shipped beside the library are thin
+ * wrappers over these calls; other languages bind them directly (ctypes, cgo, JNI).
+ *
+ * Conventions
+ *   - Every call returns an sbh_status; on failure sbh_last_error() returns a
+ *     thread-local message.
+ *   - Point, normal and query arrays passed to tree construction are row-major
+ *     [n][dim] float32, as the reference's pybind11 caster hands them to
+ *     PyQuadtree/PyOctree (include/py_tree.h:30-46).
+ *   - Query arrays passed to evaluation are structure-of-arrays [dim][nq]
+ *     float32 (x[0..nq), y[0..nq), z[0..nq)): the layout the reference copies
+ *     to the device (src/sbh_gpu.cu:217-218, read at :89-94).
+ *   - Results are float32 [nq], as the reference returns them (src/sbh_gpu.cu:244-245).
+ */
+#ifndef SBH_B200_H
+#define SBH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SBH_B200_ABI_VERSION 1
+
+typedef enum sbh_status {
+  SBH_OK = 0,
+  SBH_ERR_INVALID_ARGUMENT = 1, /* bad size, pointer, dimension or enum value */
+  SBH_ERR_CUDA = 2,             /* a CUDA runtime call failed (message has details) */
+  SBH_ERR_OUT_OF_MEMORY = 3,    /* device or host allocation failed */
+  SBH_ERR_NO_DEVICE = 4,        /* no CUDA device, or the library has no sm_100a image for it */
+  SBH_ERR_DEVICE_LIMIT = 5,     /* a device-side iteration bound was hit (corrupt tree or
+                                   input); results of that call are undefined */
+  SBH_ERR_UNSUPPORTED = 6       /* valid request this build does not serve */
+} sbh_status;
+
+/* Kernel functions.  0-2 are the reference's KernelFuncID (include/kernel.h:24-28):
+ *   GRAVITY         -m / (|p-q| + 0.1)                          (kernel.h:31-35)
+ *   WINDING_NUMBER  3D: m n.(p-q) / (4 pi (|p-q|^3 + 1e-5))      (kernel.h:46-53)
+ *                   2D: m n.(p-q) / (2 pi (|p-q|^2 + 1e-5))      (kernel.h:38-44)
+ *   SMOOTH_DIST     exp(-alpha |p-q|)   (mass ignored)           (kernel.h:55-59)
+ * 3 is new: PLUMMER  m / sqrt(|p-q|^2 + eps^2). */
+typedef enum sbh_kernel {
+  SBH_KERNEL_GRAVITY = 0,
+  SBH_KERNEL_WINDING_NUMBER = 1,
+  SBH_KERNEL_SMOOTH_DIST = 2,
+  SBH_KERNEL_PLUMMER = 3
+} sbh_kernel;
+
+typedef enum sbh_method {
+  SBH_METHOD_BRUTE_FORCE = 0, /* bruteForceSummationGPU (include/brute_force_gpu.h:18-66) */
+  SBH_METHOD_BARNES_HUT = 1,  /* per-query acceptance as evaluateBarnesHut_stackless
+                                 (include/barnes_hut.h:23-78) */
+  SBH_METHOD_BARNES_HUT_VOTE = 2, /* warp-vote acceptance over 32 consecutive queries as
+                                     evaluateBarnesHutGPUVote (include/barnes_hut_gpu.h:19-72) */
+  SBH_METHOD_STOCHASTIC = 3   /* multi-level prefix control variate sampler
+                                 (include/tree_sampler.h:21-113, tree_sampler_gpu.h:25-140) */
+} sbh_method;
+
+/* sbh_params.flags */
+#define SBH_FLAG_KEEP_ORDER 0x1u /* evaluate queries in the given order (no spatial sort) */
+
+typedef struct sbh_params {
+  int32_t method;                /* sbh_method */
+  int32_t kernel;                /* sbh_kernel */
+  float beta;                    /* Barnes-Hut opening threshold (1/theta); +inf = exact */
+  int32_t samples_per_subdomain; /* stochastic method: sampled paths per root child */
+  uint64_t seed;                 /* stochastic method: Philox key; results are a pure
+                                    function of (seed, query index) */
+  float alpha;                   /* smooth distance; NaN = the tree's alpha */
+  float eps;                     /* Plummer softening length */
+  uint32_t flags;                /* SBH_FLAG_* */
+  uint32_t reserved;
+} sbh_params;
+
+/* Fills *p with the defaults: brute force, gravity, beta 2, 1 sample per
+ * subdomain, seed 0, alpha = tree's, eps 1e-3, no flags. */
+void sbh_params_init(sbh_params* p);
+
+typedef struct sbh_tree_info {
+  int32_t dim;            /* 2 or 3 */
+  int32_t dim_split_log;  /* 1..3: branching factor 2^(dim*dim_split_log) */
+  int32_t leaf_size;      /* points per leaf at most (unless max depth is hit) */
+  int32_t max_depth;      /* depth cap of the build (the plugin uses 100) */
+  int64_t num_points;
+  int64_t num_nodes;
+  int32_t depth;          /* deepest level present */
+  int32_t root_children;  /* children of the root (subdomains of the sampler) */
+  float alpha;
+  int32_t reserved;
+  uint64_t device_bytes;  /* device bytes held by a GPU tree (0 for host trees) */
+} sbh_tree_info;
+
+typedef struct sbh_host_tree sbh_host_tree;
+typedef struct sbh_gpu_tree sbh_gpu_tree;
+
+const char* sbh_status_string(int status);
+const char* sbh_last_error(void);
+int sbh_abi_version(void);
+
+/* ---- host trees ------------------------------------------------------------
+ * Builds the reference tree (Tree2D/Tree3D, include/tree3d.h:338-371) with the
+ * same node numbering, child order, bounds, diameters, aggregates and point
+ * permutation, bit for bit.  Replaces PyQuadtree/PyOctree's constructor
+ * (include/py_tree.h:30-46, 58-74); the plugin's classes are leaf_size 1 and
+ * max_depth 100 (src/sbh.cpp:171-177, include/py_tree.h:44,72). */
+int sbh_host_tree_create(int dim, int dim_split_log, int leaf_size, int max_depth,
+                         const float* points, const float* normals, const float* masses,
+                         int64_t n, const float* min_corner, const float* max_corner,
+                         float alpha, sbh_host_tree** out);
+void sbh_host_tree_destroy(sbh_host_tree* tree);
+int sbh_host_tree_info(const sbh_host_tree* tree, sbh_tree_info* info);
+/* Copies the node arrays out (any pointer may be NULL).  child_first[v] is the
+ * buffer index of v's first child (children are contiguous, in cell order);
+ * mask is [nn][mask_words] with mask_words = max(1, branching/64); bmin/bmax
+ * are [nn][dim]; agg is [nn][2*dim+2] = mass, centroid, normal, alpha. */
+int sbh_host_tree_export_nodes(const sbh_host_tree* tree, int64_t* start, int64_t* end,
+                               int64_t* parent, int32_t* depth, int32_t* num_children,
+                               uint8_t* is_leaf, int64_t* child_first, uint64_t* mask,
+                               float* bmin, float* bmax, float* diameter, float* agg);
+/* Copies the points out in build order ([n][dim] row-major). */
+int sbh_host_tree_export_points(const sbh_host_tree* tree, float* points, float* normals,
+                                float* masses);
+
+/* ---- device-resident trees --------------------------------------------------
+ * Uploads a host tree to `device` in structure-of-arrays form.  Replaces
+ * PyQuadtreeGPU/PyOctreeGPU's constructor (include/py_tree_gpu.h:38-49, 69-80).
+ * The GPU tree does not reference the host tree after this returns. */
+int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_tree** out);
+void sbh_gpu_tree_destroy(sbh_gpu_tree* tree);
+int sbh_gpu_tree_info(const sbh_gpu_tree* tree, sbh_tree_info* info);
+
+/* ---- evaluation, host buffers (blocking) ------------------------------------
+ * queries: host [dim][nq] float32; results: host [nq] float32; contribs:
+ * optional host [nq] int32 receiving each query's number of kernel
+ * evaluations (the reference CPU plugin's counts, src/sbh.cpp:98-142);
+ * kernel_ms: optional, receives the device time of the evaluation kernels.
+ * stream: cudaStream_t or NULL for the legacy default stream.  Returns after
+ * the results are in host memory.  Replaces the 27 entry points of
+ * src/sbh_gpu.cu:212-550 (3 methods x 3 kernels x 3 tree types each). */
+int sbh_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* queries, int64_t nq,
+             float* results, int32_t* contribs, float* kernel_ms, void* stream);
+
+/* ---- evaluation, device buffers (asynchronous) -------------------------------
+ * Same computation with d_queries/d_results (and optional d_contribs) in device
+ * memory of the tree's device; enqueued on `stream`, returns without waiting.
+ * Temporary device memory comes from the stream-ordered allocator of that
+ * stream.  Device-side limit violations are reported by the next blocking call
+ * on the same tree, or by sbh_gpu_tree_check. */
+int sbh_eval_device(sbh_gpu_tree* tree, const sbh_params* params, const float* d_queries,
+                    int64_t nq, float* d_results, int32_t* d_contribs, void* stream);
+
+/* Synchronises `stream` and reports (and clears) any device-side limit
+ * violation recorded by earlier calls on this tree. */
+int sbh_gpu_tree_check(sbh_gpu_tree* tree, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SBH_B200_H */

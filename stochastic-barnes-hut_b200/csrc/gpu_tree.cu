@@ -1,0 +1,340 @@
+// C ABI: device-resident trees and evaluation entry points.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "launch.h"
+
+struct sbh_gpu_tree {
+  int device = 0;
+  int sm_count = 0;
+  sbh::DevTree dev = {};
+  void* mem = nullptr;  // one allocation: status word, points, nodes
+  size_t bytes = 0;
+  int* d_status = nullptr;
+  sbh_tree_info info = {};
+  std::mutex mu;        // serialises blocking calls (they share `ws`)
+  void* ws = nullptr;   // workspace of blocking calls
+  size_t ws_bytes = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+int cuda_fail(cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a sticky launch error so later calls are not poisoned
+  return sbh::fail(e == cudaErrorMemoryAllocation ? SBH_ERR_OUT_OF_MEMORY : SBH_ERR_CUDA,
+                   std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define SBH_CK(call, what)                          \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+int check_params(const sbh_gpu_tree* tree, const sbh_params* p, int64_t nq) {
+  if (!tree || !p) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null tree or params");
+  if (nq < 0 || nq > (int64_t)INT32_MAX)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "query count must be in [0, 2^31)");
+  if (p->method < SBH_METHOD_BRUTE_FORCE || p->method > SBH_METHOD_STOCHASTIC)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "unknown method");
+  if (p->kernel < SBH_KERNEL_GRAVITY || p->kernel > SBH_KERNEL_PLUMMER)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "unknown kernel");
+  if (p->method == SBH_METHOD_STOCHASTIC && p->samples_per_subdomain < 1)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "samples_per_subdomain must be >= 1");
+  if (p->method == SBH_METHOD_STOCHASTIC &&
+      (int64_t)tree->info.root_children * p->samples_per_subdomain > (int64_t)INT32_MAX)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "too many sampled paths per query");
+  return SBH_OK;
+}
+
+// Device bytes an evaluation needs besides queries and results: the query
+// order and the sort workspace (0 when the method keeps the given order).
+bool wants_sort(const sbh_params* p) {
+  if (p->flags & SBH_FLAG_KEEP_ORDER) return false;
+  return p->method == SBH_METHOD_BARNES_HUT || p->method == SBH_METHOD_STOCHASTIC;
+}
+
+cudaError_t run_eval(sbh_gpu_tree* tree, const sbh_params* p, const float* d_q, int64_t nq,
+                     float* d_out, int* d_contribs, int* d_order, void* d_sortws,
+                     cudaStream_t stream) {
+  const sbh::DevTree& t = tree->dev;
+  sbh::KParams kp;
+  kp.alpha = std::isnan(p->alpha) ? t.alpha : p->alpha;
+  kp.eps2 = p->eps * p->eps;
+  const int* order = nullptr;
+  if (wants_sort(p) && nq > 0) {
+    cudaError_t e = sbh::launch_query_sort(d_q, nq, t.dim, d_sortws, d_order, stream);
+    if (e != cudaSuccess) return e;
+    order = d_order;
+  }
+  switch (p->method) {
+    case SBH_METHOD_BRUTE_FORCE: {
+      cudaError_t e =
+          sbh::launch_brute_force(t, p->kernel, d_q, nq, kp, d_out, stream, tree->sm_count);
+      if (e == cudaSuccess && d_contribs) e = sbh::launch_fill_int(d_contribs, nq, (int)t.n, stream);
+      return e;
+    }
+    case SBH_METHOD_BARNES_HUT:
+    case SBH_METHOD_BARNES_HUT_VOTE:
+      return sbh::launch_barnes_hut(t, p->kernel, p->method == SBH_METHOD_BARNES_HUT_VOTE, d_q,
+                                    nq, order, p->beta, kp, d_out, d_contribs, tree->d_status,
+                                    stream);
+    case SBH_METHOD_STOCHASTIC:
+      return sbh::launch_stochastic(t, p->kernel, d_q, nq, order, p->samples_per_subdomain,
+                                    p->seed, kp, d_out, d_contribs, tree->d_status, stream,
+                                    tree->sm_count);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_tree** out) {
+  if (!out) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "out must be non-null");
+  *out = nullptr;
+  if (!host) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null host tree");
+  const sbh::HostTree& h = host->t;
+  if (h.nn > (int64_t)INT32_MAX || h.n > (int64_t)INT32_MAX)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "tree too large for 32-bit device indices");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return sbh::fail(SBH_ERR_NO_DEVICE, "no CUDA device is visible");
+  }
+  if (device < 0 || device >= ndev) return sbh::fail(SBH_ERR_NO_DEVICE, "device index out of range");
+  cudaDeviceProp prop;
+  SBH_CK(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+  if (prop.major != 10 || prop.minor != 0)
+    return sbh::fail(SBH_ERR_NO_DEVICE,
+                     std::string("this build carries sm_100a code only; device is ") + prop.name +
+                         " (sm_" + std::to_string(prop.major) + std::to_string(prop.minor) + ")");
+  DeviceGuard guard(device);
+
+  const int64_t n = h.n, nn = h.nn;
+  const int d = h.dim, mw = h.mw;
+  std::vector<float4> pt_pm(n), pt_nrm(n), nd_cm(nn), nd_agg(nn), nd_bmin(nn), nd_bmax(nn);
+  std::vector<int4> nd_topo(nn);
+  for (int64_t i = 0; i < n; i++) {
+    pt_pm[i] = make_float4(h.pos[i * d], h.pos[i * d + 1], d == 3 ? h.pos[i * d + 2] : 0.f, h.mass[i]);
+    pt_nrm[i] = make_float4(h.nrm[i * d], h.nrm[i * d + 1], d == 3 ? h.nrm[i * d + 2] : 0.f, 0.f);
+  }
+  for (int64_t v = 0; v < nn; v++) {
+    nd_cm[v] = make_float4(h.apos[v * d], h.apos[v * d + 1], d == 3 ? h.apos[v * d + 2] : 0.f, h.diam[v]);
+    nd_agg[v] = make_float4(h.amass[v], h.anrm[v * d], h.anrm[v * d + 1], d == 3 ? h.anrm[v * d + 2] : 0.f);
+    nd_bmin[v] = make_float4(h.bmin[v * d], h.bmin[v * d + 1], d == 3 ? h.bmin[v * d + 2] : 0.f, 0.f);
+    nd_bmax[v] = make_float4(h.bmax[v * d], h.bmax[v * d + 1], d == 3 ? h.bmax[v * d + 2] : 0.f, 0.f);
+    nd_topo[v] = make_int4(h.leaf[v] ? 0 : (int)h.first_child[v], h.leaf[v] ? 0 : h.nch[v],
+                           (int)h.start[v], (int)h.end[v]);
+  }
+
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    size_t o = off;
+    off += align256(b > 0 ? b : 1);
+    return o;
+  };
+  const size_t o_status = take(sizeof(int));
+  const size_t o_pm = take(n * sizeof(float4)), o_nrm = take(n * sizeof(float4));
+  const size_t o_cm = take(nn * sizeof(float4)), o_agg = take(nn * sizeof(float4));
+  const size_t o_topo = take(nn * sizeof(int4));
+  const size_t o_bmin = take(nn * sizeof(float4)), o_bmax = take(nn * sizeof(float4));
+  const size_t o_mask = take((size_t)nn * mw * sizeof(uint64_t));
+
+  sbh_gpu_tree* g = new (std::nothrow) sbh_gpu_tree();
+  if (!g) return sbh::fail(SBH_ERR_OUT_OF_MEMORY, "host allocation failed");
+  g->device = device;
+  g->sm_count = prop.multiProcessorCount;
+  g->bytes = off;
+  cudaError_t e = cudaMalloc(&g->mem, off);
+  if (e != cudaSuccess) {
+    delete g;
+    return cuda_fail(e, "cudaMalloc(tree)");
+  }
+  char* base = static_cast<char*>(g->mem);
+  struct Copy {
+    size_t off;
+    const void* src;
+    size_t bytes;
+  } copies[] = {{o_pm, pt_pm.data(), n * sizeof(float4)},
+                {o_nrm, pt_nrm.data(), n * sizeof(float4)},
+                {o_cm, nd_cm.data(), nn * sizeof(float4)},
+                {o_agg, nd_agg.data(), nn * sizeof(float4)},
+                {o_topo, nd_topo.data(), nn * sizeof(int4)},
+                {o_bmin, nd_bmin.data(), nn * sizeof(float4)},
+                {o_bmax, nd_bmax.data(), nn * sizeof(float4)},
+                {o_mask, h.mask.data(), (size_t)nn * mw * sizeof(uint64_t)}};
+  e = cudaMemset(base + o_status, 0, sizeof(int));
+  for (const Copy& c : copies)
+    if (e == cudaSuccess && c.bytes) e = cudaMemcpy(base + c.off, c.src, c.bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaEventCreate(&g->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&g->ev1);
+  if (e != cudaSuccess) {
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    cudaFree(g->mem);
+    delete g;
+    return cuda_fail(e, "tree upload");
+  }
+  g->d_status = reinterpret_cast<int*>(base + o_status);
+  sbh::DevTree& t = g->dev;
+  t.pt_pm = reinterpret_cast<const float4*>(base + o_pm);
+  t.pt_nrm = reinterpret_cast<const float4*>(base + o_nrm);
+  t.nd_cm = reinterpret_cast<const float4*>(base + o_cm);
+  t.nd_agg = reinterpret_cast<const float4*>(base + o_agg);
+  t.nd_topo = reinterpret_cast<const int4*>(base + o_topo);
+  t.nd_bmin = reinterpret_cast<const float4*>(base + o_bmin);
+  t.nd_bmax = reinterpret_cast<const float4*>(base + o_bmax);
+  t.nd_mask = reinterpret_cast<const unsigned long long*>(base + o_mask);
+  t.n = n;
+  t.nn = nn;
+  t.dim = d;
+  t.dsl = h.dsl;
+  t.ds = h.ds;
+  t.bf = h.bf;
+  t.mw = mw;
+  t.depth = h.depth;
+  t.root_children = (nn > 0 && !h.leaf[0]) ? h.nch[0] : 0;
+  t.alpha = h.alpha;
+  sbh::fill_info(h, &g->info);
+  g->info.device_bytes = off;
+  *out = g;
+  return sbh::ok();
+}
+
+SBH_API void sbh_gpu_tree_destroy(sbh_gpu_tree* tree) {
+  if (!tree) return;
+  {
+    DeviceGuard guard(tree->device);
+    cudaDeviceSynchronize();
+    if (tree->ws) cudaFree(tree->ws);
+    if (tree->mem) cudaFree(tree->mem);
+    if (tree->ev0) cudaEventDestroy(tree->ev0);
+    if (tree->ev1) cudaEventDestroy(tree->ev1);
+  }
+  delete tree;
+}
+
+SBH_API int sbh_gpu_tree_info(const sbh_gpu_tree* tree, sbh_tree_info* info) {
+  if (!tree || !info) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null argument");
+  *info = tree->info;
+  return sbh::ok();
+}
+
+SBH_API int sbh_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* queries,
+                     int64_t nq, float* results, int32_t* contribs, float* kernel_ms,
+                     void* stream_ptr) {
+  int st = check_params(tree, params, nq);
+  if (st != SBH_OK) return st;
+  if (nq > 0 && (!queries || !results))
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
+  if (kernel_ms) *kernel_ms = 0.f;
+  if (nq == 0) return sbh::ok();
+  std::lock_guard<std::mutex> lock(tree->mu);
+  DeviceGuard guard(tree->device);
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  const int dim = tree->dev.dim;
+  const size_t b_q = align256((size_t)dim * nq * sizeof(float));
+  const size_t b_out = align256((size_t)nq * sizeof(float));
+  const size_t b_cnt = contribs ? align256((size_t)nq * sizeof(int)) : 0;
+  const size_t b_ord = align256((size_t)nq * sizeof(int));
+  const size_t b_sort = align256(sbh::query_sort_workspace_bytes(nq));
+  const size_t need = b_q + b_out + b_cnt + b_ord + b_sort;
+  if (tree->ws_bytes < need) {
+    if (tree->ws) cudaFree(tree->ws);
+    tree->ws = nullptr;
+    tree->ws_bytes = 0;
+    SBH_CK(cudaMalloc(&tree->ws, need), "cudaMalloc(workspace)");
+    tree->ws_bytes = need;
+  }
+  char* w = static_cast<char*>(tree->ws);
+  float* d_q = reinterpret_cast<float*>(w);
+  float* d_out = reinterpret_cast<float*>(w + b_q);
+  int* d_cnt = contribs ? reinterpret_cast<int*>(w + b_q + b_out) : nullptr;
+  int* d_ord = reinterpret_cast<int*>(w + b_q + b_out + b_cnt);
+  void* d_sort = w + b_q + b_out + b_cnt + b_ord;
+
+  SBH_CK(cudaMemcpyAsync(d_q, queries, (size_t)dim * nq * sizeof(float), cudaMemcpyHostToDevice, stream),
+         "copy queries to device");
+  SBH_CK(cudaEventRecord(tree->ev0, stream), "cudaEventRecord");
+  SBH_CK(run_eval(tree, params, d_q, nq, d_out, d_cnt, d_ord, d_sort, stream), "kernel launch");
+  SBH_CK(cudaEventRecord(tree->ev1, stream), "cudaEventRecord");
+  SBH_CK(cudaMemcpyAsync(results, d_out, (size_t)nq * sizeof(float), cudaMemcpyDeviceToHost, stream),
+         "copy results to host");
+  if (contribs)
+    SBH_CK(cudaMemcpyAsync(contribs, d_cnt, (size_t)nq * sizeof(int), cudaMemcpyDeviceToHost, stream),
+           "copy counts to host");
+  int status = 0;
+  SBH_CK(cudaMemcpyAsync(&status, tree->d_status, sizeof(int), cudaMemcpyDeviceToHost, stream),
+         "read status");
+  SBH_CK(cudaStreamSynchronize(stream), "evaluation");
+  if (kernel_ms) SBH_CK(cudaEventElapsedTime(kernel_ms, tree->ev0, tree->ev1), "cudaEventElapsedTime");
+  if (status != 0) {
+    cudaMemsetAsync(tree->d_status, 0, sizeof(int), stream);
+    cudaStreamSynchronize(stream);
+    return sbh::fail(SBH_ERR_DEVICE_LIMIT, "device traversal hit a bound (status bits " +
+                                               std::to_string(status) + ")");
+  }
+  return sbh::ok();
+}
+
+SBH_API int sbh_eval_device(sbh_gpu_tree* tree, const sbh_params* params, const float* d_queries,
+                            int64_t nq, float* d_results, int32_t* d_contribs, void* stream_ptr) {
+  int st = check_params(tree, params, nq);
+  if (st != SBH_OK) return st;
+  if (nq == 0) return sbh::ok();
+  if (!d_queries || !d_results)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
+  DeviceGuard guard(tree->device);
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  void* tmp = nullptr;
+  int* d_ord = nullptr;
+  void* d_sort = nullptr;
+  if (wants_sort(params)) {
+    const size_t b_ord = align256((size_t)nq * sizeof(int));
+    SBH_CK(cudaMallocAsync(&tmp, b_ord + sbh::query_sort_workspace_bytes(nq), stream),
+           "cudaMallocAsync(workspace)");
+    d_ord = static_cast<int*>(tmp);
+    d_sort = static_cast<char*>(tmp) + b_ord;
+  }
+  cudaError_t e = run_eval(tree, params, d_queries, nq, d_results, d_contribs, d_ord, d_sort, stream);
+  if (tmp) cudaFreeAsync(tmp, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  return sbh::ok();
+}
+
+SBH_API int sbh_gpu_tree_check(sbh_gpu_tree* tree, void* stream_ptr) {
+  if (!tree) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null tree");
+  DeviceGuard guard(tree->device);
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  int status = 0;
+  SBH_CK(cudaMemcpyAsync(&status, tree->d_status, sizeof(int), cudaMemcpyDeviceToHost, stream),
+         "read status");
+  SBH_CK(cudaStreamSynchronize(stream), "synchronise");
+  if (status != 0) {
+    SBH_CK(cudaMemsetAsync(tree->d_status, 0, sizeof(int), stream), "clear status");
+    SBH_CK(cudaStreamSynchronize(stream), "synchronise");
+    return sbh::fail(SBH_ERR_DEVICE_LIMIT, "device traversal hit a bound (status bits " +
+                                               std::to_string(status) + ")");
+  }
+  return sbh::ok();
+}

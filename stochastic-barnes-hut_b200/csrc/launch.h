@@ -1,0 +1,30 @@
+// Host-side launchers of the summation kernels (internal to libsbh_b200.so).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+
+namespace sbh {
+
+cudaError_t launch_brute_force(const DevTree& t, int kernel, const float* q, long long nq,
+                               const KParams& kp, float* out, cudaStream_t stream, int sm_count);
+
+cudaError_t launch_barnes_hut(const DevTree& t, int kernel, bool vote, const float* q,
+                              long long nq, const int* order, float beta, const KParams& kp,
+                              float* out, int* contribs, int* status, cudaStream_t stream);
+
+cudaError_t launch_stochastic(const DevTree& t, int kernel, const float* q, long long nq,
+                              const int* order, int samples, unsigned long long seed,
+                              const KParams& kp, float* out, int* contribs, int* status,
+                              cudaStream_t stream, int sm_count);
+
+// Spatial ordering of queries: order[i] is the i-th query in Morton-bucket
+// order.  `ws` must hold query_sort_workspace_bytes(nq) bytes.
+size_t query_sort_workspace_bytes(long long nq);
+cudaError_t launch_query_sort(const float* q, long long nq, int dim, void* ws, int* order,
+                              cudaStream_t stream);
+
+cudaError_t launch_fill_int(int* p, long long n, int value, cudaStream_t stream);
+
+}  // namespace sbh

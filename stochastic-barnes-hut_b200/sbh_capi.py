@@ -1,0 +1,226 @@
+"""ctypes binding of the C ABI in include/sbh_b200.h (libsbh_b200.so).
+
+This is the language-neutral boundary of the library: host trees, device
+trees and the evaluation calls, with plain pointers and sizes.  The pybind11
+modules `sbh` / `sbh_gpu` cover the reference's Python surface; this module is
+for callers that hold raw buffers (device pointers from PyTorch, CuPy, another
+runtime) and is what the parity tests call.
+
+Importing this module loads the library and raises if it is missing: there is
+no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsbh_b200.so")
+
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_CUDA = 2
+ERR_OUT_OF_MEMORY = 3
+ERR_NO_DEVICE = 4
+ERR_DEVICE_LIMIT = 5
+ERR_UNSUPPORTED = 6
+
+GRAVITY, WINDING_NUMBER, SMOOTH_DIST, PLUMMER = 0, 1, 2, 3
+BRUTE_FORCE, BARNES_HUT, BARNES_HUT_VOTE, STOCHASTIC = 0, 1, 2, 3
+FLAG_KEEP_ORDER = 0x1
+
+# Every function the header declares, with its ctypes signature.
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_SIGNATURES = {
+    "sbh_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "sbh_last_error": (ctypes.c_char_p, []),
+    "sbh_abi_version": (ctypes.c_int, []),
+    "sbh_params_init": (None, [_P]),
+    "sbh_host_tree_create": (ctypes.c_int, [ctypes.c_int] * 4 + [_P, _P, _P, _I64, _P, _P,
+                                                                 ctypes.c_float, _P]),
+    "sbh_host_tree_destroy": (None, [_P]),
+    "sbh_host_tree_info": (ctypes.c_int, [_P, _P]),
+    "sbh_host_tree_export_nodes": (ctypes.c_int, [_P] * 13),
+    "sbh_host_tree_export_points": (ctypes.c_int, [_P] * 4),
+    "sbh_gpu_tree_create": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+    "sbh_gpu_tree_destroy": (None, [_P]),
+    "sbh_gpu_tree_info": (ctypes.c_int, [_P, _P]),
+    "sbh_eval": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P]),
+    "sbh_eval_device": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
+    "sbh_gpu_tree_check": (ctypes.c_int, [_P, _P]),
+}
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int32), ("kernel", ctypes.c_int32), ("beta", ctypes.c_float),
+                ("samples_per_subdomain", ctypes.c_int32), ("seed", ctypes.c_uint64),
+                ("alpha", ctypes.c_float), ("eps", ctypes.c_float), ("flags", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+class TreeInfo(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int32), ("dim_split_log", ctypes.c_int32),
+                ("leaf_size", ctypes.c_int32), ("max_depth", ctypes.c_int32),
+                ("num_points", ctypes.c_int64), ("num_nodes", ctypes.c_int64),
+                ("depth", ctypes.c_int32), ("root_children", ctypes.c_int32),
+                ("alpha", ctypes.c_float), ("reserved", ctypes.c_int32),
+                ("device_bytes", ctypes.c_uint64)]
+
+
+class SbhError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `make -C {HERE}`")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def _check(status: int):
+    if status != OK:
+        l = lib()
+        msg = (l.sbh_last_error() or b"").decode() or l.sbh_status_string(status).decode()
+        raise SbhError(status, msg)
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def params(method=BRUTE_FORCE, kernel=GRAVITY, beta=2.0, samples_per_subdomain=1, seed=0,
+           alpha=None, eps=1e-3, flags=0) -> Params:
+    p = Params()
+    lib().sbh_params_init(ctypes.byref(p))
+    p.method, p.kernel, p.beta = method, kernel, beta
+    p.samples_per_subdomain, p.seed = samples_per_subdomain, seed
+    p.alpha = math.nan if alpha is None else alpha
+    p.eps, p.flags = eps, flags
+    return p
+
+
+class HostTree:
+    """sbh_host_tree_*: the reference tree built on the host."""
+
+    def __init__(self, points, normals, masses, min_corner, max_corner, alpha=1.0,
+                 dim_split_log=1, leaf_size=1, max_depth=100):
+        pts = np.ascontiguousarray(points, np.float32)
+        if pts.ndim != 2:
+            raise ValueError("points must be (n, dim)")
+        n, dim = pts.shape
+        nrm = np.ascontiguousarray(normals, np.float32).reshape(n, dim)
+        m = np.ascontiguousarray(masses, np.float32).reshape(n)
+        lo = np.ascontiguousarray(min_corner, np.float32).reshape(dim)
+        hi = np.ascontiguousarray(max_corner, np.float32).reshape(dim)
+        h = ctypes.c_void_p()
+        _check(lib().sbh_host_tree_create(dim, dim_split_log, leaf_size, max_depth, _ptr(pts),
+                                          _ptr(nrm), _ptr(m), n, _ptr(lo), _ptr(hi),
+                                          ctypes.c_float(alpha), ctypes.byref(h)))
+        self.handle = h
+
+    def info(self) -> TreeInfo:
+        i = TreeInfo()
+        _check(lib().sbh_host_tree_info(self.handle, ctypes.byref(i)))
+        return i
+
+    def export_nodes(self) -> dict:
+        i = self.info()
+        nn, d = i.num_nodes, i.dim
+        mw = max(1, (1 << (d * i.dim_split_log)) >> 6)
+        out = dict(start=np.zeros(nn, np.int64), end=np.zeros(nn, np.int64),
+                   parent=np.zeros(nn, np.int64), depth=np.zeros(nn, np.int32),
+                   num_children=np.zeros(nn, np.int32), is_leaf=np.zeros(nn, np.uint8),
+                   first_child=np.zeros(nn, np.int64), mask=np.zeros((nn, mw), np.uint64),
+                   bmin=np.zeros((nn, d), np.float32), bmax=np.zeros((nn, d), np.float32),
+                   diameter=np.zeros(nn, np.float32), agg=np.zeros((nn, 2 * d + 2), np.float32))
+        keys = ["start", "end", "parent", "depth", "num_children", "is_leaf", "first_child",
+                "mask", "bmin", "bmax", "diameter", "agg"]
+        _check(lib().sbh_host_tree_export_nodes(self.handle, *[_ptr(out[k]) for k in keys]))
+        return out
+
+    def export_points(self) -> dict:
+        i = self.info()
+        out = dict(points=np.zeros((i.num_points, i.dim), np.float32),
+                   normals=np.zeros((i.num_points, i.dim), np.float32),
+                   masses=np.zeros(i.num_points, np.float32))
+        _check(lib().sbh_host_tree_export_points(self.handle, _ptr(out["points"]),
+                                                 _ptr(out["normals"]), _ptr(out["masses"])))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sbh_host_tree_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+
+class GpuTree:
+    """sbh_gpu_tree_*: a tree resident in device memory."""
+
+    def __init__(self, host: HostTree, device: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().sbh_gpu_tree_create(host.handle, device, ctypes.byref(h)))
+        self.handle = h
+        i = TreeInfo()
+        _check(lib().sbh_gpu_tree_info(h, ctypes.byref(i)))
+        self.info = i
+        self.dim = i.dim
+
+    def eval(self, queries, p: Params, stream: int = 0, contribs: bool = False):
+        """Blocking evaluation of host queries (n, dim): returns (values, kernel_ms[, counts])."""
+        q = np.asfortranarray(queries, np.float32)
+        if q.ndim != 2 or q.shape[1] != self.dim:
+            raise ValueError(f"queries must be (n, {self.dim})")
+        nq = q.shape[0]
+        out = np.zeros(nq, np.float32)
+        cnt = np.zeros(nq, np.int32) if contribs else None
+        ms = ctypes.c_float(0)
+        _check(lib().sbh_eval(self.handle, ctypes.byref(p), _ptr(q), nq, _ptr(out), _ptr(cnt),
+                              ctypes.byref(ms), ctypes.c_void_p(stream)))
+        return (out, ms.value, cnt) if contribs else (out, ms.value)
+
+    def eval_host_ptr(self, q_ptr: int, nq: int, out_ptr: int, p: Params, stream: int = 0,
+                      contribs_ptr: int = 0) -> float:
+        """Blocking evaluation with raw host pointers (SoA [dim][nq] queries)."""
+        ms = ctypes.c_float(0)
+        _check(lib().sbh_eval(self.handle, ctypes.byref(p), ctypes.c_void_p(q_ptr), nq,
+                              ctypes.c_void_p(out_ptr), ctypes.c_void_p(contribs_ptr or None),
+                              ctypes.byref(ms), ctypes.c_void_p(stream)))
+        return ms.value
+
+    def eval_device(self, d_queries: int, nq: int, d_results: int, p: Params, stream: int = 0,
+                    d_contribs: int = 0):
+        """Asynchronous evaluation on device pointers (SoA [dim][nq] float32 queries)."""
+        _check(lib().sbh_eval_device(self.handle, ctypes.byref(p), ctypes.c_void_p(d_queries), nq,
+                                     ctypes.c_void_p(d_results),
+                                     ctypes.c_void_p(d_contribs or None), ctypes.c_void_p(stream)))
+
+    def check(self, stream: int = 0):
+        _check(lib().sbh_gpu_tree_check(self.handle, ctypes.c_void_p(stream)))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sbh_gpu_tree_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()

@@ -1,0 +1,54 @@
+"""The C ABI library loads and exports every function include/sbh_b200.h declares,
+and the pybind11 modules expose the reference plugin's names.  No GPU needed."""
+import ctypes
+import os
+import re
+
+import sbh
+import sbh_capi as C
+import sbh_gpu
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "sbh_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sbh_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported():
+    lib = ctypes.CDLL(C.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert missing == []
+
+
+def test_ctypes_binding_covers_the_header():
+    assert sorted(C._SIGNATURES) == declared_functions()
+
+
+def test_struct_layouts():
+    assert ctypes.sizeof(C.Params) == 40
+    assert ctypes.sizeof(C.TreeInfo) == 56
+    assert C.lib().sbh_abi_version() == 1
+
+
+def test_status_strings():
+    assert C.lib().sbh_status_string(0) == b"ok"
+    assert C.lib().sbh_status_string(5) == b"device-side iteration limit hit"
+
+
+def test_reference_plugin_surface():
+    for cls in ("QuadtreeGPU1", "QuadtreeGPU2", "QuadtreeGPU3", "OctreeGPU1", "OctreeGPU2",
+                "OctreeGPU3"):
+        assert hasattr(sbh_gpu, cls)
+    for k in ("gravity", "wn", "smoothdist"):
+        for f in ("eval_brute_force_", "eval_barnes_hut_", "multi_level_prefix_control_variate_"):
+            assert hasattr(sbh_gpu, f + k)
+        assert hasattr(sbh, "eval_barnes_hut_" + k)
+        assert hasattr(sbh, "multi_level_prefix_control_variate_" + k)
+    for cls in ("Quadtree1", "Quadtree2", "Quadtree3", "Octree1", "Octree2", "Octree3"):
+        assert hasattr(sbh, cls)
