@@ -1,0 +1,443 @@
+"""Benchmark of the stochastic Barnes-Hut summation path on B200.
+
+Default workload (the configuration the headline metric is quoted on):
+stochastic Barnes-Hut winding number in 3D -- 1,048,576 oriented points sampled
+area-uniformly on a torus (R=0.6, r=0.2) with exact normals and area weights
+4 pi^2 R r / N, an Octree2-type tree (branching 64, leaf size 1, the reference's
+recommended tree for the sampler), 4,194,304 queries uniform in [-1,1]^3, and a
+budget of 256 sampled paths per query (samples_per_subdomain = 256 / root
+children).  A step is one evaluation of all queries.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sbh_wn|bh_wn|plain_small_bf|plain_small_bh]
+
+`value` is queries/s with queries already resident in HBM (device-pointer C ABI
+call: Morton bucketing + sampler kernel), timed with CUDA events per step, L2
+flushed between steps.  `e2e` is the same through the blocking C ABI call with
+pinned host buffers (host->device copy, evaluation, device->host copy inside
+the timed region).  Under torchrun every rank evaluates its own query batch
+against its own replica of the tree (replicas only: the path has no exchange
+step); `value` is all ranks' queries over the slowest rank's time.
+
+`--impl reference` times the reference's own CPU implementation
+(src/sbh.cpp multiLevelPrefixControlVariateSampler, compiled unmodified in
+oracle/_ref) on the same workload, on bounded query samples, with all host
+threads; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "stochastic-barnes-hut_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "served vs plain-BH queries/s at 1e-3 med rel err (FP64 ref); p50/p99 ms"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 512 << 20
+
+WORKLOADS = {
+    # name: (description, method, kernel, n points, n queries, tree kind, budget/beta)
+    "sbh_wn": dict(desc="stochastic BH winding number, torus 1,048,576 pts, 4,194,304 queries, "
+                        "Octree2 (branching 64, leaf 1), 256 sampled paths/query",
+                   method="stochastic", kernel="wn", n=1 << 20, nq=1 << 22, dsl=2, leaf=1,
+                   budget=256, source="torus"),
+    "bh_wn": dict(desc="deterministic BH winding number, torus 1,048,576 pts, 4,194,304 queries, "
+                       "Octree1 (branching 8, leaf 1), theta 0.5",
+                  method="barnes_hut", kernel="wn", n=1 << 20, nq=1 << 22, dsl=1, leaf=1,
+                  beta=2.0, source="torus"),
+    "plain_small_bf": dict(desc="brute-force Plummer potential (eps 1e-3), 65,536 Gaussian-mixture "
+                                "sources x 65,536 queries", method="brute_force",
+                           kernel="plummer", n=65536, nq=65536, dsl=1, leaf=8, source="gauss"),
+    "plain_small_bh": dict(desc="deterministic BH Plummer potential (eps 1e-3), 65,536 "
+                                "Gaussian-mixture sources x 65,536 queries, theta 0.5, leaf 8",
+                           method="barnes_hut", kernel="plummer", n=65536, nq=65536, dsl=1,
+                           leaf=8, beta=2.0, source="gauss"),
+}
+
+
+def load_peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def make_inputs(wl, rank=0):
+    import sbh_workloads as W
+    if wl["source"] == "torus":
+        pts, nrm, m = W.torus_surface(wl["n"], seed=2024)
+    else:
+        pts, nrm, m = W.gaussian_mixture(wl["n"], seed=2024)
+    lo, hi = W.padded_box(pts)
+    q = W.uniform_queries(wl["nq"], seed=4048 + rank)
+    return pts, nrm, m, lo, hi, q
+
+
+def kernel_id(C, name):
+    return {"gravity": C.GRAVITY, "wn": C.WINDING_NUMBER, "smooth": C.SMOOTH_DIST,
+            "plummer": C.PLUMMER}[name]
+
+
+def method_id(C, name):
+    return {"brute_force": C.BRUTE_FORCE, "barnes_hut": C.BARNES_HUT,
+            "stochastic": C.STOCHASTIC}[name]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.rows = []
+        self.proc = None
+        self.dev = device_index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(args, wl):
+    import torch
+
+    import sbh_capi as C
+    import sbh_workloads as W
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    s_handle = stream.cuda_stream
+
+    pts, nrm, m, lo, hi, q = make_inputs(wl, rank)
+    t0 = time.perf_counter()
+    host = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=wl["dsl"], leaf_size=wl["leaf"])
+    build_s = time.perf_counter() - t0
+    gpu = C.GpuTree(host, device=local)
+    info = gpu.info
+    nq = q.shape[0]
+    samples = W.samples_for_budget(wl.get("budget", 1), info.root_children)
+    p = C.params(method=method_id(C, wl["method"]), kernel=kernel_id(C, wl["kernel"]),
+                 beta=wl.get("beta", 2.0), samples_per_subdomain=samples, seed=1234)
+
+    d_q = torch.from_numpy(np.ascontiguousarray(q.T)).to(dev)  # SoA [3][nq]
+    d_out = torch.empty(nq, dtype=torch.float32, device=dev)
+    d_cnt = torch.empty(nq, dtype=torch.int32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def step_device():
+        gpu.eval_device(d_q.data_ptr(), nq, d_out.data_ptr(), p, stream=s_handle)
+
+    # Work counts (untimed): contributions per query define the algorithmic bytes.
+    gpu.eval_device(d_q.data_ptr(), nq, d_out.data_ptr(), p, stream=s_handle,
+                    d_contribs=d_cnt.data_ptr())
+    gpu.check(s_handle)
+    contribs = d_cnt.to(torch.int64).sum().item()
+
+    # Device-resident timing.
+    for _ in range(args.warmup):
+        flush.zero_()
+        step_device()
+    gpu.check(s_handle)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    times = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step_device()
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    gpu.check(s_handle)
+    step_ms = [a.elapsed_time(b) for a, b in times]
+    total_ms = float(sum(step_ms))
+
+    # Dominant kernel alone: the sampler on pre-bucketed queries (no sort launch).
+    order = morton_order(q)
+    d_qs = torch.from_numpy(np.ascontiguousarray(q[order].T)).to(dev)
+    pk = C.params(method=p.method, kernel=p.kernel, beta=p.beta, samples_per_subdomain=samples,
+                  seed=p.seed, flags=C.FLAG_KEEP_ORDER)
+    for _ in range(max(1, args.warmup)):
+        flush.zero_()
+        gpu.eval_device(d_qs.data_ptr(), nq, d_out.data_ptr(), pk, stream=s_handle)
+    kern_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        gpu.eval_device(d_qs.data_ptr(), nq, d_out.data_ptr(), pk, stream=s_handle)
+        e1.record(stream)
+        kern_ms.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    kern_ms = [a.elapsed_time(b) for a, b in kern_ms]
+
+    # End to end through the blocking C ABI call with pinned host buffers.
+    h_q = torch.from_numpy(np.ascontiguousarray(q.T)).pin_memory()
+    h_out = torch.empty(nq, dtype=torch.float32).pin_memory()
+    for _ in range(args.warmup):
+        gpu.eval_host_ptr(h_q.data_ptr(), nq, h_out.data_ptr(), p, stream=s_handle)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e2e = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        gpu.eval_host_ptr(h_q.data_ptr(), nq, h_out.data_ptr(), p, stream=s_handle)
+        e1.record(stream)
+        e2e.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    e2e_ms = float(sum(a.elapsed_time(b) for a, b in e2e))
+
+    if dist:
+        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_ms = t.tolist()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+
+    bytes_per_eval = 32 if wl["kernel"] == "wn" else 16
+    alg_bytes = contribs * bytes_per_eval + nq * 16
+    kmean_s = statistics.mean(kern_ms) / 1e3
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / kmean_s / 1e9
+    launches_per_step = {"stochastic": 6, "barnes_hut": 6, "brute_force": 1}[wl["method"]]
+    clk = clocks.summary()
+    out = {
+        "metric": METRIC,
+        "value": world * nq / (total_ms / 1e3 / args.steps),
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generators; the reference publishes no dataset)",
+        "config": {
+            "workload": wl["desc"],
+            "method": wl["method"], "kernel": wl["kernel"], "points": wl["n"],
+            "queries_per_gpu": nq, "tree": f"dim 3, dim_split_log {wl['dsl']}, leaf {wl['leaf']}",
+            "tree_nodes": info.num_nodes, "root_children": info.root_children,
+            "samples_per_subdomain": samples if wl["method"] == "stochastic" else None,
+            "paths_per_query": samples * info.root_children if wl["method"] == "stochastic" else None,
+            "beta": wl.get("beta"),
+            "mean_kernel_evals_per_query": contribs / nq,
+            "host_build_s": round(build_s, 3),
+            "l2": "512 MiB buffer written between timed steps; tree+queries exceed L2 as well",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        },
+        "e2e": {"value": world * nq / (e2e_ms / 1e3 / args.steps), "unit": "queries/s",
+                "h2d_bytes_per_step": nq * 12, "d2h_bytes_per_step": nq * 4,
+                "ms_per_step": e2e_ms / args.steps},
+        "roofline": {
+            "bound": "hbm", "kernel": "stochastic_kernel" if wl["method"] == "stochastic" else wl["method"],
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+            "kernel_ms": statistics.mean(kern_ms),
+            "algorithmic_bytes": alg_bytes,
+            "bytes_definition": f"{bytes_per_eval} B per kernel evaluation (source or node record) + 16 B per query",
+            "traffic": None,
+        },
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        out["cpu_baseline"] = cpu_baseline(wl, pts, nrm, m, lo, hi, q, samples,
+                                           budget_s=args.cpu_seconds)
+    return out
+
+
+def morton_order(q):
+    lo, hi = q.min(0), q.max(0)
+    c = np.clip(((q - lo) / np.maximum(hi - lo, 1e-30) * 64).astype(np.int64), 0, 63)
+    key = np.zeros(len(q), np.int64)
+    for b in range(6):
+        for d in range(3):
+            key |= ((c[:, d] >> b) & 1) << (3 * b + d)
+    return np.argsort(key, kind="stable")
+
+
+def cpu_baseline(wl, pts, nrm, m, lo, hi, q, samples, budget_s=20.0):
+    """The reference's CPU plugin on a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.ref_available():
+        return {"value": None, "unit": "queries/s", "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    t = O.RefTree(pts, nrm, m, lo, hi, dim_split_log=wl["dsl"], leaf_size=wl["leaf"])
+    kid = {"gravity": 0, "wn": 1, "smooth": 2}.get(wl["kernel"])
+    cores = O.ref_hardware_concurrency()
+    # Probe with a small sample, then size the timed sample to ~budget_s.
+    n0 = 512
+    secs = run_ref(t, wl, kid, q[:n0], samples)
+    n = int(min(len(q), max(n0, n0 * budget_s / max(secs, 1e-3))))
+    secs = run_ref(t, wl, kid, q[:n], samples)
+    return {"value": n / secs, "unit": "queries/s", "cores": cores, "kind": "reference",
+            "sample": f"first {n} of the {len(q)} queries, same tree and parameters, "
+                      f"{secs:.1f} s, src/sbh.cpp thread pool ({cores} threads)"}
+
+
+def run_ref(t, wl, kid, q, samples):
+    if wl["method"] == "stochastic":
+        _, _, secs = t.plugin_sbh(kid, q, samples)
+    elif wl["method"] == "barnes_hut":
+        if kid is None:
+            t0 = time.perf_counter()
+            t.bh(3, q, wl.get("beta", 2.0))
+            return time.perf_counter() - t0
+        _, secs = t.plugin_bh(kid, q, wl.get("beta", 2.0))
+    else:  # brute force: the reference CPU path is Barnes-Hut with beta = inf
+        if kid is None:
+            t0 = time.perf_counter()
+            t.bh(3, q, np.inf)
+            return time.perf_counter() - t0
+        _, secs = t.plugin_bh(kid, q, np.inf)
+    return secs
+
+
+def run_reference(args, wl):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import sbh_workloads as W
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libsbh_ref.so is not built"}
+    pts, nrm, m, lo, hi, q = make_inputs(wl, 0)
+    t = O.RefTree(pts, nrm, m, lo, hi, dim_split_log=wl["dsl"], leaf_size=wl["leaf"])
+    info_children = int((t.dump().parent == 0).sum() - 1) if wl["n"] <= 200000 else None
+    if info_children is None:
+        import sbh_capi as C
+        info_children = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=wl["dsl"],
+                                   leaf_size=wl["leaf"]).info().root_children
+    samples = W.samples_for_budget(wl.get("budget", 1), info_children)
+    kid = {"gravity": 0, "wn": 1, "smooth": 2}.get(wl["kernel"])
+    cores = O.ref_hardware_concurrency()
+    per_step = max(64, args.ref_sample)
+    secs = run_ref(t, wl, kid, q[:64], samples)
+    per_step = int(min(per_step, max(64, 64 * args.ref_step_seconds / max(secs, 1e-3))))
+    for i in range(args.warmup):
+        run_ref(t, wl, kid, q[:min(per_step, 256)], samples)
+    total = 0.0
+    for i in range(args.steps):
+        lo_i = (i * per_step) % max(1, len(q) - per_step)
+        total += run_ref(t, wl, kid, q[lo_i:lo_i + per_step], samples)
+    value = args.steps * per_step / total
+    sample = (f"{per_step} queries per step of the {len(q)}-query workload, "
+              f"src/sbh.cpp thread pool ({cores} threads), tree build excluded")
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": wl["desc"], "samples_per_subdomain": samples},
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sbh_wn")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-sample", type=int, default=4096)
+    ap.add_argument("--ref-step-seconds", type=float, default=4.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    wl = WORKLOADS[args.workload]
+    out = run_reference(args, wl) if args.impl == "reference" else run_ours(args, wl)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

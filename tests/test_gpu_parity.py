@@ -204,7 +204,7 @@ def test_sampler_variance_matches_reference():
     _, var_gpu = _replicate_stats(gpu, q, C.WINDING_NUMBER, 2, reps)
     ot = O.OracleTree(pts, nrm, m, lo, hi, dim_split_log=2)
     qq = np.tile(q, (reps, 1))
-    seeds = np.arange(len(qq), dtype=np.uint32) * 2654435761 % (2**32)
+    seeds = (np.arange(len(qq), dtype=np.uint64) * 2654435761 % (2**32)).astype(np.uint32)
     # The oracle's std::mt19937 sampler is the reference's own (pinned bit for bit).
     rv, _ = ot.sbh(O.WINDING_NUMBER, qq, 2, rng=O.RNG_MT19937, mt_seeds=seeds.astype(np.uint32))
     var_ref = rv.reshape(reps, len(q)).astype(np.float64).var(0, ddof=1)
