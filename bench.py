@@ -430,10 +430,14 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-sample", type=int, default=4096)
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
+    ap.add_argument("--nq", type=int, default=0, help="override the query count (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.nq:
+        wl["nq"] = args.nq
+        wl["desc"] += f" [query count overridden: {args.nq}]"
     out = run_reference(args, wl) if args.impl == "reference" else run_ours(args, wl)
     if out is not None:
         print(json.dumps(out), flush=True)
