@@ -157,6 +157,32 @@ int sbh_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* queries,
 int sbh_eval_device(sbh_gpu_tree* tree, const sbh_params* params, const float* d_queries,
                     int64_t nq, float* d_results, int32_t* d_contribs, void* stream);
 
+/* ---- evaluation without device allocation -----------------------------------
+ * No counterpart in the reference: its plugin allocates and frees device
+ * buffers inside every call (src/sbh_gpu.cu:217-222).
+ * Same computation and arguments as sbh_eval_device, but the call allocates
+ * nothing: the query-ordering scratch of the Barnes-Hut and stochastic methods
+ * comes from one fixed array compiled into the library (about 3 MiB, which
+ * every GPU that loads the library holds until the process exits) instead of
+ * cudaMallocAsync.  It is meant for callers that cannot allocate device memory
+ * while they run -- a serving loop that reserves its whole HBM budget at
+ * start-up and must not allocate per request (an allocation can stall or fail
+ * under memory pressure at any moment), or code whose device memory belongs to
+ * another allocator's budget, such as a framework's caching allocator.
+ * Limits and rules:
+ *   - at most SBH_STATIC_SCRATCH_MAX_QUERIES queries per call; larger counts
+ *     return SBH_ERR_INVALID_ARGUMENT (split the batch);
+ *   - the first call on a device looks up the array's device address with that
+ *     device current; make that first call before any stream capture begins;
+ *   - all calls share the one array and it keeps the previous call's contents
+ *     (each call re-initialises what it reads), so calls that overlap on the
+ *     GPU -- on different streams or from different threads -- race: order
+ *     them on one stream or wait between them. */
+#define SBH_STATIC_SCRATCH_MAX_QUERIES 262144
+int sbh_eval_device_static_scratch(sbh_gpu_tree* tree, const sbh_params* params,
+                                   const float* d_queries, int64_t nq, float* d_results,
+                                   int32_t* d_contribs, void* stream);
+
 /* Synchronises `stream` and reports (and clears) any device-side limit
  * violation recorded by earlier calls on this tree. */
 int sbh_gpu_tree_check(sbh_gpu_tree* tree, void* stream);

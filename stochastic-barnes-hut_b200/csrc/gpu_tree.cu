@@ -338,3 +338,67 @@ SBH_API int sbh_gpu_tree_check(sbh_gpu_tree* tree, void* stream_ptr) {
   }
   return sbh::ok();
 }
+
+// ---- evaluation without device allocation -----------------------------------
+// sbh_eval_device allocates the query-ordering scratch of the Barnes-Hut and
+// stochastic methods per call (cudaMallocAsync).  The entry point below takes
+// that scratch from a fixed device array in this library's image instead, for
+// callers that must not allocate device memory once they are running.
+
+static __device__ __align__(256) unsigned char g_static_scratch[
+    ((size_t)SBH_STATIC_SCRATCH_MAX_QUERIES * sizeof(int) + 255) / 256 * 256 +  // query order
+    256 + ((size_t)1 << 18) * 4 + (size_t)SBH_STATIC_SCRATCH_MAX_QUERIES * 4];  // sort workspace
+
+namespace {
+
+constexpr size_t kStaticOrderBytes =
+    ((size_t)SBH_STATIC_SCRATCH_MAX_QUERIES * sizeof(int) + 255) / 256 * 256;
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+void* g_static_addr[kStaticMaxDevices] = {};
+
+// Device address of g_static_scratch on the current device `dev`, resolved once
+// per device (the host-side name of a __device__ variable is not a device address).
+int static_scratch_address(int dev, char** out) {
+  if (dev < 0 || dev >= kStaticMaxDevices)
+    return sbh::fail(SBH_ERR_UNSUPPORTED, "device index beyond the static scratch table");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+    g_static_addr[dev] = p;
+  }
+  *out = static_cast<char*>(g_static_addr[dev]);
+  return SBH_OK;
+}
+
+}  // namespace
+
+SBH_API int sbh_eval_device_static_scratch(sbh_gpu_tree* tree, const sbh_params* params,
+                                           const float* d_queries, int64_t nq,
+                                           float* d_results, int32_t* d_contribs,
+                                           void* stream_ptr) {
+  int st = check_params(tree, params, nq);
+  if (st != SBH_OK) return st;
+  if (nq > (int64_t)SBH_STATIC_SCRATCH_MAX_QUERIES)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT,
+                     "sbh_eval_device_static_scratch takes at most " +
+                         std::to_string((long long)SBH_STATIC_SCRATCH_MAX_QUERIES) +
+                         " queries per call; got " + std::to_string((long long)nq));
+  if (nq == 0) return sbh::ok();
+  if (!d_queries || !d_results)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
+  if (sbh::query_sort_workspace_bytes(nq) + kStaticOrderBytes > sizeof(g_static_scratch))
+    return sbh::fail(SBH_ERR_UNSUPPORTED, "static scratch is smaller than the sort workspace");
+  DeviceGuard guard(tree->device);
+  char* scratch = nullptr;
+  st = static_scratch_address(tree->device, &scratch);
+  if (st != SBH_OK) return st;
+  int* d_ord = reinterpret_cast<int*>(scratch);
+  void* d_sort = scratch + kStaticOrderBytes;
+  cudaError_t e = run_eval(tree, params, d_queries, nq, d_results, d_contribs, d_ord, d_sort,
+                           static_cast<cudaStream_t>(stream_ptr));
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  return sbh::ok();
+}

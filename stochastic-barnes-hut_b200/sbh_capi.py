@@ -52,7 +52,11 @@ _SIGNATURES = {
     "sbh_eval": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P]),
     "sbh_eval_device": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
     "sbh_gpu_tree_check": (ctypes.c_int, [_P, _P]),
+    "sbh_eval_device_static_scratch": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
 }
+
+# Largest query count sbh_eval_device_static_scratch accepts per call.
+STATIC_SCRATCH_MAX_QUERIES = 262144
 
 
 class Params(ctypes.Structure):
@@ -213,6 +217,16 @@ class GpuTree:
         _check(lib().sbh_eval_device(self.handle, ctypes.byref(p), ctypes.c_void_p(d_queries), nq,
                                      ctypes.c_void_p(d_results),
                                      ctypes.c_void_p(d_contribs or None), ctypes.c_void_p(stream)))
+
+    def eval_device_static_scratch(self, d_queries: int, nq: int, d_results: int, p: Params,
+                                   stream: int = 0, d_contribs: int = 0):
+        """As eval_device, without any device allocation: scratch comes from a fixed
+        array in the library (at most STATIC_SCRATCH_MAX_QUERIES queries per call;
+        calls that overlap on the GPU race on that array)."""
+        _check(lib().sbh_eval_device_static_scratch(
+            self.handle, ctypes.byref(p), ctypes.c_void_p(d_queries), nq,
+            ctypes.c_void_p(d_results), ctypes.c_void_p(d_contribs or None),
+            ctypes.c_void_p(stream)))
 
     def check(self, stream: int = 0):
         _check(lib().sbh_gpu_tree_check(self.handle, ctypes.c_void_p(stream)))
