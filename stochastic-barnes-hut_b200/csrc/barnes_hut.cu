@@ -70,22 +70,23 @@ __global__ void __launch_bounds__(BH_THREADS)
       stk[sp - 1].cur = e.cur + 1;
     }
     const bool in = (e.mask >> lane) & 1u;
+    // Topology and node record in one round trip (a one-point leaf's record is
+    // its point).
     const int4 topo = __ldg(t.nd_topo + node);
+    const float4 cm = __ldg(t.nd_cm + node);
     const bool leaf = topo.y == 0;
-    float4 cm = make_float4(0.f, 0.f, 0.f, 0.f);
     bool acc = false;
     if (leaf) {
       acc = in && (__int_as_float(0x7f800000) >= beta);
-    } else {
-      cm = __ldg(t.nd_cm + node);
-      if (in) acc = far_field_ratio<DIM>(cm, q) >= beta;
+    } else if (in) {
+      acc = far_field_ratio<DIM>(cm, q) >= beta;
     }
     if (VOTE) {
       const unsigned rej = __ballot_sync(0xffffffffu, in && !acc);
       acc = in && rej == 0u;
     }
     if (acc) {
-      if (leaf) {
+      if (leaf && topo.w - topo.z != 1) {
         for (int i = topo.z; i < topo.w; i++) {
           total = radd(total, kernel_exact<DIM, K>(__ldg(t.pt_pm + i), __ldg(t.pt_nrm + i), q, kp));
           nc++;

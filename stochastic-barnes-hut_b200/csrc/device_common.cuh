@@ -11,6 +11,8 @@ namespace sbh {
 //           pt_nrm [n]  float4 (nx, ny, nz, 0)
 //   nodes   nd_cm  [nn] float4 (centroid x, y, z, diameter)
 //           nd_agg [nn] float4 (mass, normal x, y, z)      aggregate LeafData
+//           (a leaf holding exactly one point stores that point's position,
+//           mass and normal instead of its aggregate)
 //           nd_topo[nn] int4   (first child, #children (0 = leaf), start, end)
 //           nd_bmin/nd_bmax [nn] float4 AABB corners (sampler only)
 //           nd_mask[nn][mw] uint64 child-cell bitmask       (sampler only)

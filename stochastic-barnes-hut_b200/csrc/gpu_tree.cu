@@ -140,8 +140,18 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
     pt_nrm[i] = make_float4(h.nrm[i * d], h.nrm[i * d + 1], d == 3 ? h.nrm[i * d + 2] : 0.f, 0.f);
   }
   for (int64_t v = 0; v < nn; v++) {
-    nd_cm[v] = make_float4(h.apos[v * d], h.apos[v * d + 1], d == 3 ? h.apos[v * d + 2] : 0.f, h.diam[v]);
-    nd_agg[v] = make_float4(h.amass[v], h.anrm[v * d], h.anrm[v * d + 1], d == 3 ? h.anrm[v * d + 2] : 0.f);
+    // A leaf's aggregate is never evaluated -- the reference sums a leaf's points
+    // (include/barnes_hut.h:40-46, tree_sampler.h:268-274) -- so a one-point leaf
+    // carries the point itself: kernels then read a node's topology and its
+    // evaluation data in one round trip.
+    if (h.leaf[v] && h.end[v] - h.start[v] == 1) {
+      const int64_t i = h.start[v];
+      nd_cm[v] = make_float4(h.pos[i * d], h.pos[i * d + 1], d == 3 ? h.pos[i * d + 2] : 0.f, h.diam[v]);
+      nd_agg[v] = make_float4(h.mass[i], h.nrm[i * d], h.nrm[i * d + 1], d == 3 ? h.nrm[i * d + 2] : 0.f);
+    } else {
+      nd_cm[v] = make_float4(h.apos[v * d], h.apos[v * d + 1], d == 3 ? h.apos[v * d + 2] : 0.f, h.diam[v]);
+      nd_agg[v] = make_float4(h.amass[v], h.anrm[v * d], h.anrm[v * d + 1], d == 3 ? h.anrm[v * d + 2] : 0.f);
+    }
     nd_bmin[v] = make_float4(h.bmin[v * d], h.bmin[v * d + 1], d == 3 ? h.bmin[v * d + 2] : 0.f, 0.f);
     nd_bmax[v] = make_float4(h.bmax[v * d], h.bmax[v * d + 1], d == 3 ? h.bmax[v * d + 2] : 0.f, 0.f);
     nd_topo[v] = make_int4(h.leaf[v] ? 0 : (int)h.first_child[v], h.leaf[v] ? 0 : h.nch[v],

@@ -169,9 +169,9 @@ class HostTree:
         return out
 
     def close(self):
-        if getattr(self, "handle", None):
-            lib().sbh_host_tree_destroy(self.handle)
-            self.handle = None
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.sbh_host_tree_destroy(self.handle)
+        self.handle = None
 
     def __del__(self):
         self.close()
@@ -232,9 +232,9 @@ class GpuTree:
         _check(lib().sbh_gpu_tree_check(self.handle, ctypes.c_void_p(stream)))
 
     def close(self):
-        if getattr(self, "handle", None):
-            lib().sbh_gpu_tree_destroy(self.handle)
-            self.handle = None
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.sbh_gpu_tree_destroy(self.handle)
+        self.handle = None
 
     def __del__(self):
         self.close()
