@@ -265,6 +265,13 @@ def run_ours(args, wl):
     torch.cuda.synchronize(dev)
     e2e_ms = float(sum(a.elapsed_time(b) for a, b in e2e))
 
+    # Accuracy on a query subset against brute force, and the deterministic
+    # Barnes-Hut comparison the workload prescribes (Octree1, theta 0.3/0.5/0.8).
+    accuracy = compare = None
+    if not args.no_accuracy:
+        accuracy, compare = accuracy_report(C, torch, wl, gpu, p, pts, nrm, m, lo, hi, d_q, nq,
+                                            s_handle, args)
+
     if dist:
         t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -321,10 +328,77 @@ def run_ours(args, wl):
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }
+    if accuracy is not None:
+        out["accuracy"] = accuracy
+        out["compare"] = compare
     if not args.no_cpu_baseline and world == 1:
         out["cpu_baseline"] = cpu_baseline(wl, pts, nrm, m, lo, hi, q, samples,
                                            budget_s=args.cpu_seconds)
     return out
+
+
+ACCURACY_SUBSET = 65536
+
+
+def rel_errors(kernel, est, ref):
+    """Per-query relative error.  The winding number vanishes outside the
+    surface, so its error is taken relative to max(|ref|, 1) (its natural unit:
+    the jump across the surface); the potentials never vanish."""
+    est = est.astype(np.float64)
+    if kernel == "wn":
+        return np.abs(est - ref) / np.maximum(np.abs(ref), 1.0)
+    return np.abs(est - ref) / np.abs(ref)
+
+
+def accuracy_report(C, torch, wl, gpu, p, pts, nrm, m, lo, hi, d_q, nq, s_handle, args):
+    dev = d_q.device
+    n_sub = min(ACCURACY_SUBSET, nq)
+    d_sub = d_q[:, :n_sub].contiguous()
+    ref = torch.empty(n_sub, dtype=torch.float32, device=dev)
+    kid = kernel_id(C, wl["kernel"])
+    gpu.eval_device(d_sub.data_ptr(), n_sub, ref.data_ptr(),
+                    C.params(method=C.BRUTE_FORCE, kernel=kid), stream=s_handle)
+    est = torch.empty(n_sub, dtype=torch.float32, device=dev)
+    gpu.eval_device(d_sub.data_ptr(), n_sub, est.data_ptr(), p, stream=s_handle)
+    torch.cuda.synchronize(dev)
+    ref_np = ref.cpu().numpy().astype(np.float64)
+    e = rel_errors(wl["kernel"], est.cpu().numpy(), ref_np)
+    accuracy = {"median_rel_err": float(np.median(e)), "p99_rel_err": float(np.percentile(e, 99)),
+                "subset_queries": n_sub,
+                "reference": "compensated FP32 brute force (within 1e-6 of FP64 by test)",
+                "definition": ("|est-ref|/max(|ref|,1)" if wl["kernel"] == "wn"
+                               else "|est-ref|/|ref|")}
+    compare = {}
+    if wl["method"] != "stochastic":
+        return accuracy, compare
+    host1 = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=1, leaf_size=1)
+    gpu1 = C.GpuTree(host1, device=dev.index or 0)
+    out = torch.empty(nq, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for theta in (0.3, 0.5, 0.8):
+        pb = C.params(method=C.BARNES_HUT, kernel=kid, beta=1.0 / theta)
+        for _ in range(3):
+            flush.zero_()
+            gpu1.eval_device(d_q.data_ptr(), nq, out.data_ptr(), pb, stream=s_handle)
+        times = []
+        for _ in range(max(3, args.steps // 4)):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            gpu1.eval_device(d_q.data_ptr(), nq, out.data_ptr(), pb, stream=s_handle)
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize(dev)
+        ms = statistics.mean(a.elapsed_time(b) for a, b in times)
+        eb = rel_errors(wl["kernel"], out[:n_sub].cpu().numpy(), ref_np)
+        compare[f"barnes_hut_theta_{theta}"] = {
+            "tree": "dim_split_log 1 (branching 8), leaf 1", "queries_per_s": nq / (ms / 1e3),
+            "ms_per_step": ms, "median_rel_err": float(np.median(eb)),
+            "p99_rel_err": float(np.percentile(eb, 99))}
+    gpu1.check(s_handle)
+    return accuracy, compare
 
 
 def morton_order(q):
@@ -427,6 +501,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sbh_wn")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-sample", type=int, default=4096)
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
