@@ -157,6 +157,83 @@ int sbh_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* queries,
 int sbh_eval_device(sbh_gpu_tree* tree, const sbh_params* params, const float* d_queries,
                     int64_t nq, float* d_results, int32_t* d_contribs, void* stream);
 
+/* ---- batched evaluation ------------------------------------------------------
+ * No counterpart in the reference, which makes one launch (and one pair of
+ * host-device copies) per call.  Evaluates many requests -- any trees resident
+ * on one device, any methods, kernels, parameters and query counts -- in one
+ * fixed pipeline captured once as a CUDA graph: Morton bucketing of all
+ * requests' queries together, then one persistent work-queue kernel.  Per
+ * request the results equal sbh_eval_device's: Barnes-Hut bit for bit, the
+ * sampler because its random streams are keyed by (seed, query index within the
+ * request).  Enqueued on `stream`; the call first waits for the previous batch
+ * of the same device to leave the staging buffers it reuses. */
+typedef struct sbh_batch_item {
+  sbh_gpu_tree* tree;
+  sbh_params params;
+  const float* d_queries;    /* device [dim][nq] float32 */
+  int64_t nq;
+  float* d_results;          /* device [nq] */
+  int32_t* d_contribs;       /* device [nq] or NULL */
+  const float* d_self_mass;  /* device [nq] or NULL: when the queries are the sources
+                                themselves, subtract each query's own term
+                                (a source of this mass at the query point) */
+} sbh_batch_item;
+int sbh_eval_batch(const sbh_batch_item* items, int n_items, void* stream);
+
+/* ---- serving ---------------------------------------------------------------
+ * No counterpart in the reference.  A server keeps trees resident on one
+ * device and evaluates requests submitted from any thread with continuous
+ * batching: `slots` batches are in flight at once (one stream each); whenever
+ * a slot is free, the requests waiting at that moment -- up to the slot's query
+ * capacity, which is the HBM admitted per batch -- form its next batch, so
+ * requests arriving while others run on the GPU are admitted as slots free up
+ * and overlap on the device.  Requests larger than a slot are split across
+ * batches.  Per request, results equal sbh_eval's (same rule as batches). */
+typedef struct sbh_server sbh_server;
+
+typedef struct sbh_server_config {
+  int32_t device;
+  int32_t slots;                   /* batches in flight (default 3) */
+  int64_t slot_queries;            /* queries admitted per batch (default 1 << 20) */
+  int32_t max_requests_per_batch;  /* default 4096 */
+  int32_t reserved;
+} sbh_server_config;
+
+typedef struct sbh_request_info {
+  int32_t status;      /* SBH_OK, or the error that ended the request */
+  int32_t batches;     /* batches the request was spread over */
+  int64_t nq;
+  double queue_ms;     /* submission to the launch of its first batch */
+  double latency_ms;   /* submission to results in host memory */
+} sbh_request_info;
+
+typedef struct sbh_server_stats {
+  int64_t requests;
+  int64_t queries;
+  int64_t batches;
+  double busy_ms;      /* wall time with at least one batch in flight */
+} sbh_server_stats;
+
+void sbh_server_config_init(sbh_server_config* cfg);
+int sbh_server_create(const sbh_server_config* cfg, sbh_server** out);
+/* Uploads a host tree and keeps it resident; *tree_id names it in requests. */
+int sbh_server_add_tree(sbh_server* server, const sbh_host_tree* host, int32_t* tree_id);
+/* Queues a request.  queries: host [dim][nq] float32; results: host [nq];
+ * contribs: optional host [nq].  The buffers must stay valid until
+ * sbh_server_wait reports the request finished. */
+int sbh_server_submit(sbh_server* server, int32_t tree_id, const sbh_params* params,
+                      const float* queries, int64_t nq, float* results, int32_t* contribs,
+                      uint64_t* request_id);
+/* Waits up to timeout_ms (< 0: forever) for a request; returns SBH_OK with
+ * *info filled when it finished (info->status holds its own outcome), or
+ * SBH_ERR_UNSUPPORTED when the wait timed out.  A finished request is
+ * forgotten after the wait that reports it. */
+int sbh_server_wait(sbh_server* server, uint64_t request_id, double timeout_ms,
+                    sbh_request_info* info);
+int sbh_server_stats_get(sbh_server* server, sbh_server_stats* stats);
+/* Finishes every queued request, then frees the server and its trees. */
+void sbh_server_destroy(sbh_server* server);
+
 /* ---- evaluation without device allocation -----------------------------------
  * No counterpart in the reference: its plugin allocates and frees device
  * buffers inside every call (src/sbh_gpu.cu:217-222).

@@ -1,0 +1,375 @@
+// Batched evaluation: a list of requests -- each its own tree, method, kernel,
+// parameters and query count -- runs as one fixed pipeline of four kernels,
+// captured once as a CUDA graph:
+//
+//   batch_keys_kernel     Morton bucket of every query of every request, inside
+//                         its tree's root box, with a per-request bucket count
+//                         sized to the request (about 8 queries per bucket);
+//   batch_scan_kernel     one exclusive scan over all requests' buckets (each
+//                         request's buckets follow the previous request's, so
+//                         the scan also places every request at its offset);
+//   batch_scatter_kernel  the sorted position of every query;
+//   batch_eval_kernel     a persistent kernel: warps take work units (32 queries
+//                         of a Barnes-Hut or brute-force request, or a pair of
+//                         sampler queries) from an atomic counter and run the
+//                         same device routines as the single-call kernels
+//                         (tasks.cuh), dispatching on method, kernel and
+//                         dimension per unit.
+//
+// Every launch parameter of the graph is fixed (grids are persistent; sizes and
+// the request table live in device memory, refreshed by one host-to-device copy
+// before each launch), so one instantiated graph serves every batch.  Results
+// are per request identical to a single call: Barnes-Hut is exact per query and
+// the sampler's random streams are keyed by (seed, query index in its request).
+#include <algorithm>
+#include <cstring>
+
+#include "batch.h"
+#include "tasks.cuh"
+
+namespace sbh {
+namespace {
+
+constexpr int kEvalThreads = 128;
+constexpr int kEvalWarps = kEvalThreads / 32;
+constexpr int kAuxThreads = 256;
+constexpr int kScanThreads = 1024;
+
+__device__ __forceinline__ int find_item_by(const BatchItem* items, int n, long long v,
+                                            long long BatchItem::*field) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].*field <= v) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ unsigned spread(unsigned v, int bits, int stride) {
+  unsigned r = 0;
+  for (int b = 0; b < bits; b++) r |= ((v >> b) & 1u) << (stride * b);
+  return r;
+}
+
+__global__ void batch_keys_kernel(const BatchHeader* __restrict__ hdr,
+                                  const BatchItem* __restrict__ items, unsigned* keys,
+                                  unsigned* hist) {
+  const int n = hdr->n_items;
+  const long long total = hdr->total_queries;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const BatchItem& it = items[find_item_by(items, n, g, &BatchItem::sort_base)];
+    const long long i = g - it.sort_base;
+    unsigned key = 0;
+    const int bits = it.sort_bits;
+    if (bits > 0) {
+      const float cells = (float)(1 << bits);
+      const int dim = it.dim;
+      unsigned c[3] = {0u, 0u, 0u};
+      for (int d = 0; d < dim; d++) {
+        const float ext = it.box_hi[d] - it.box_lo[d];
+        float f = ext > 0.f ? (it.q[d * it.nq + i] - it.box_lo[d]) * (cells / ext) : 0.f;
+        f = f == f ? fminf(fmaxf(f, 0.f), cells - 1.f) : 0.f;
+        c[d] = (unsigned)f;
+      }
+      key = dim == 3 ? (spread(c[0], bits, 3) | (spread(c[1], bits, 3) << 1) |
+                        (spread(c[2], bits, 3) << 2))
+                     : (spread(c[0], bits, 2) | (spread(c[1], bits, 2) << 1));
+    }
+    const unsigned bucket = (unsigned)(it.bucket_base + key);
+    keys[g] = bucket;
+    atomicAdd(hist + bucket, 1u);
+  }
+}
+
+// Exclusive scan of hist[0, total_buckets) by one block.
+__global__ void __launch_bounds__(kScanThreads)
+    batch_scan_kernel(const BatchHeader* __restrict__ hdr, unsigned* hist) {
+  __shared__ unsigned s[kScanThreads];
+  const long long total = hdr->total_buckets;
+  const long long per = (total + kScanThreads - 1) / kScanThreads;
+  const long long b = threadIdx.x * per, e = min(total, b + per);
+  unsigned sum = 0;
+  for (long long k = b; k < e; k++) sum += hist[k];
+  s[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < kScanThreads; off <<= 1) {
+    const unsigned v = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
+    __syncthreads();
+    s[threadIdx.x] += v;
+    __syncthreads();
+  }
+  unsigned run = s[threadIdx.x] - sum;
+  for (long long k = b; k < e; k++) {
+    const unsigned c = hist[k];
+    hist[k] = run;
+    run += c;
+  }
+}
+
+__global__ void batch_scatter_kernel(const BatchHeader* __restrict__ hdr,
+                                     const BatchItem* __restrict__ items,
+                                     const unsigned* __restrict__ keys, unsigned* hist,
+                                     int* order) {
+  const int n = hdr->n_items;
+  const long long total = hdr->total_queries;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const BatchItem& it = items[find_item_by(items, n, g, &BatchItem::sort_base)];
+    const unsigned pos = atomicAdd(hist + keys[g], 1u);
+    order[pos] = (int)(g - it.sort_base);
+  }
+}
+
+constexpr int kTreeWords = (int)((sizeof(DevTree) + 15) / 16 * 4);
+
+// One work unit of each method, as separate functions so each is register
+// allocated on its own (the dispatcher below stays small).
+template <int DIM, int K, bool VOTE>
+__device__ __noinline__ void run_bh(const DevTree& t, const BatchItem& it, long long u,
+                                    const int* ord, float* scratch, int stack_cap, int* status) {
+  const long long s0 = u * kUnitQueriesWarp;
+  const long long s1 = min(it.nq, s0 + kUnitQueriesWarp);
+  bh_warp_task<DIM, K, VOTE>(t, it.q, it.nq, ord, s0, s1, it.beta, it.kp, it.out, it.contribs,
+                             status, reinterpret_cast<BhStackEntry*>(scratch), stack_cap,
+                             it.self_mass);
+}
+
+template <int DIM, int K>
+__device__ __noinline__ void run_sbh(const DevTree& t, const BatchItem& it, long long u,
+                                     const int* ord, float* scratch, int* status) {
+  const int lane = threadIdx.x & 31;
+  const SbhWarpSmem ws = sbh_carve(scratch, t.root_children);
+  const long long s0 = u * kUnitQueriesSampler;
+  const long long s1 = min(it.nq, s0 + kUnitQueriesSampler);
+  for (long long s = s0; s < s1; s++) {
+    const long long qi = ord ? (long long)__ldg(ord + s) : s;
+    const float3 q = load_query<DIM>(it.q, it.nq, qi);
+    float r;
+    int c;
+    sbh_query<DIM, K>(t, q, it.query_base + qi, it.samples, it.seed, it.kp, ws, status, r, c);
+    if (lane == 0) {
+      if (it.self_mass) r = rsub(r, self_term<DIM, K>(q, __ldg(it.self_mass + qi), it.kp));
+      it.out[qi] = r;
+      if (it.contribs) it.contribs[qi] = c;
+    }
+  }
+}
+
+template <int DIM, int K>
+__device__ __noinline__ void run_bf(const DevTree& t, const BatchItem& it, long long u) {
+  const long long s0 = u * kUnitQueriesWarp;
+  bf_warp_task<DIM, K>(t, it.q, it.nq, s0, min(it.nq, s0 + kUnitQueriesWarp), it.kp, it.out,
+                       it.contribs, it.self_mass);
+}
+
+template <int DIM, int K>
+__device__ __forceinline__ void run_unit(const DevTree& t, const BatchItem& it, long long u,
+                                         const int* order, float* scratch, int stack_cap,
+                                         int* status) {
+  const int* ord = it.sort_bits > 0 ? order + it.sort_base : nullptr;
+  switch (it.method) {
+    case 1: run_bh<DIM, K, false>(t, it, u, ord, scratch, stack_cap, status); break;
+    case 2: run_bh<DIM, K, true>(t, it, u, ord, scratch, stack_cap, status); break;
+    case 3: run_sbh<DIM, K>(t, it, u, ord, scratch, status); break;
+    default: run_bf<DIM, K>(t, it, u); break;
+  }
+}
+
+__global__ void __launch_bounds__(kEvalThreads, 8)
+    batch_eval_kernel(BatchHeader* hdr, const BatchItem* __restrict__ items,
+                      const DevTree* __restrict__ trees, const int* __restrict__ order,
+                      int* status, int warp_words, int stack_cap) {
+  extern __shared__ float4 s_eval[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  float* wbase = reinterpret_cast<float*>(s_eval) + (size_t)warp * warp_words;
+  DevTree& t = *reinterpret_cast<DevTree*>(wbase);
+  float* scratch = wbase + kTreeWords;
+  const int n = hdr->n_items;
+  const long long total = hdr->total_units;
+  int cached_tree = -1;
+  for (;;) {
+    unsigned long long unit = 0;
+    if (lane == 0) unit = atomicAdd(&hdr->next_unit, 1ull);
+    unit = __shfl_sync(0xffffffffu, unit, 0);
+    if ((long long)unit >= total) break;
+    const int item = find_item_by(items, n, (long long)unit, &BatchItem::unit_base);
+    const BatchItem& it = items[item];
+    if (it.tree != cached_tree) {
+      __syncwarp();
+      const int* src = reinterpret_cast<const int*>(trees + it.tree);
+      int* dst = reinterpret_cast<int*>(wbase);
+      for (int w = lane; w < (int)(sizeof(DevTree) / 4); w += 32) dst[w] = __ldg(src + w);
+      cached_tree = it.tree;
+      __syncwarp();
+    }
+    const long long u = (long long)unit - it.unit_base;
+    const int key = (t.dim == 3 ? 0 : 4) + it.kernel;
+    switch (key) {
+      case 0: run_unit<3, kGravity>(t, it, u, order, scratch, stack_cap, status); break;
+      case 1: run_unit<3, kWindingNumber>(t, it, u, order, scratch, stack_cap, status); break;
+      case 2: run_unit<3, kSmoothDist>(t, it, u, order, scratch, stack_cap, status); break;
+      case 3: run_unit<3, kPlummer>(t, it, u, order, scratch, stack_cap, status); break;
+      case 4: run_unit<2, kGravity>(t, it, u, order, scratch, stack_cap, status); break;
+      case 5: run_unit<2, kWindingNumber>(t, it, u, order, scratch, stack_cap, status); break;
+      case 6: run_unit<2, kSmoothDist>(t, it, u, order, scratch, stack_cap, status); break;
+      default: run_unit<2, kPlummer>(t, it, u, order, scratch, stack_cap, status); break;
+    }
+    __syncwarp();
+  }
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+long long max_buckets(const BatchEngine::Limits& lim) {
+  return lim.max_queries / 8 + 2LL * lim.max_items + 1024;
+}
+
+int sort_bits_for(long long nq, int dim) {
+  // About 8 queries per bucket; 6 bits per axis (3D) / 9 (2D) at most.
+  if (nq < 64) return 0;
+  int bits = 0;
+  const int cap = dim == 3 ? 6 : 9;
+  while (bits < cap && (1LL << (dim * (bits + 1))) * 8 <= nq) bits++;
+  return bits;
+}
+
+}  // namespace
+
+BatchEngine::BatchEngine(const Limits& lim, int sm_count) : lim_(lim), sm_count_(sm_count) {
+  const long long nb = max_buckets(lim_);
+  const size_t o_hdr = 0;
+  const size_t o_items = o_hdr + align256(sizeof(BatchHeader));
+  const size_t o_keys = o_items + align256(sizeof(BatchItem) * lim_.max_items);
+  const size_t o_hist = o_keys + align256(sizeof(unsigned) * lim_.max_queries);
+  const size_t o_order = o_hist + align256(sizeof(unsigned) * nb);
+  dev_bytes_ = o_order + align256(sizeof(int) * lim_.max_queries);
+  if (cudaMalloc(&dev_, dev_bytes_) != cudaSuccess) {
+    dev_ = nullptr;
+    return;
+  }
+  char* b = static_cast<char*>(dev_);
+  d_header_ = reinterpret_cast<BatchHeader*>(b + o_hdr);
+  d_items_ = reinterpret_cast<BatchItem*>(b + o_items);
+  d_keys_ = reinterpret_cast<unsigned*>(b + o_keys);
+  d_hist_ = reinterpret_cast<unsigned*>(b + o_hist);
+  d_order_ = reinterpret_cast<int*>(b + o_order);
+  if (cudaMallocHost(&h_stage_, o_keys) != cudaSuccess) h_stage_ = nullptr;
+  // Per-warp shared memory: the tree record, then the larger of the
+  // Barnes-Hut stack and the sampler's scratch.
+  const int stack_words = (lim_.max_tree_depth + 2) * (int)sizeof(BhStackEntry) / 4;
+  const int scratch = std::max(stack_words, sbh_warp_words(lim_.max_root_children));
+  const int warp_words = kTreeWords + (scratch + 3) / 4 * 4;
+  eval_smem_ = (size_t)kEvalWarps * warp_words * sizeof(float);
+  if (eval_smem_ > 48 * 1024)
+    cudaFuncSetAttribute(batch_eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)eval_smem_);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_eval_kernel, kEvalThreads,
+                                                eval_smem_);
+  eval_blocks_ = std::max(1, per_sm) * sm_count_;
+}
+
+BatchEngine::~BatchEngine() {
+  if (exec_) cudaGraphExecDestroy(exec_);
+  if (h_stage_) cudaFreeHost(h_stage_);
+  if (dev_) cudaFree(dev_);
+}
+
+std::string BatchEngine::plan(std::vector<BatchItem>& items,
+                              const std::vector<DevTree>& host_trees) const {
+  if (!dev_ || !h_stage_) return "batch engine has no device or pinned memory";
+  if ((int)items.size() > lim_.max_items) return "too many requests in one batch";
+  long long sort_base = 0, bucket_base = 0, unit_base = 0;
+  for (BatchItem& it : items) {
+    if (it.tree < 0 || it.tree >= (int)host_trees.size()) return "request names an unknown tree";
+    const DevTree& t = host_trees[it.tree];
+    if (t.depth + 2 > lim_.max_tree_depth + 2) return "tree deeper than the engine supports";
+    if (t.root_children > lim_.max_root_children) return "tree root wider than the engine supports";
+    const bool sorted = it.method == 1 || it.method == 3;  // vote keeps the caller's order
+    it.sort_bits = (sorted && it.sort_bits >= 0) ? sort_bits_for(it.nq, t.dim) : 0;
+    it.dim = t.dim;
+    it.sort_base = sort_base;
+    it.bucket_base = bucket_base;
+    it.buckets = it.sort_bits > 0 ? (1LL << (t.dim * it.sort_bits)) : 1;
+    it.unit_base = unit_base;
+    const long long per_unit = it.method == 3 ? kUnitQueriesSampler : kUnitQueriesWarp;
+    it.units = (it.nq + per_unit - 1) / per_unit;
+    sort_base += it.nq;
+    bucket_base += it.buckets;
+    unit_base += it.units;
+  }
+  if (sort_base > lim_.max_queries) return "batch exceeds the engine's query capacity";
+  if (bucket_base > max_buckets(lim_)) return "batch exceeds the engine's bucket capacity";
+  return "";
+}
+
+cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status) {
+  if (exec_) {
+    cudaGraphExecDestroy(exec_);
+    exec_ = nullptr;
+  }
+  // Captured on a private stream (the caller's may be the legacy default
+  // stream, which cannot be captured); the graph is launched on the caller's.
+  cudaStream_t stream = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return e;
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(stream);
+    return e;
+  }
+  const int aux_blocks = sm_count_ * 4;
+  const int stack_cap = lim_.max_tree_depth + 2;
+  const int stack_words = stack_cap * (int)sizeof(BhStackEntry) / 4;
+  const int scratch = std::max(stack_words, sbh_warp_words(lim_.max_root_children));
+  const int warp_words = kTreeWords + (scratch + 3) / 4 * 4;
+  cudaMemsetAsync(d_hist_, 0, sizeof(unsigned) * max_buckets(lim_), stream);
+  batch_keys_kernel<<<aux_blocks, kAuxThreads, 0, stream>>>(d_header_, d_items_, d_keys_, d_hist_);
+  batch_scan_kernel<<<1, kScanThreads, 0, stream>>>(d_header_, d_hist_);
+  batch_scatter_kernel<<<aux_blocks, kAuxThreads, 0, stream>>>(d_header_, d_items_, d_keys_,
+                                                              d_hist_, d_order_);
+  batch_eval_kernel<<<eval_blocks_, kEvalThreads, eval_smem_, stream>>>(
+      d_header_, d_items_, d_trees, d_order_, d_status, warp_words, stack_cap);
+  e = cudaStreamEndCapture(stream, &graph);
+  cudaStreamDestroy(stream);
+  if (e != cudaSuccess) return e;
+  e = cudaGraphInstantiate(&exec_, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    exec_ = nullptr;
+    return e;
+  }
+  captured_trees_ = d_trees;
+  captured_status_ = d_status;
+  return cudaSuccess;
+}
+
+cudaError_t BatchEngine::launch(const std::vector<BatchItem>& items, const DevTree* d_trees,
+                                int* d_status, cudaStream_t stream) {
+  if (!dev_ || !h_stage_) return cudaErrorMemoryAllocation;
+  if (!exec_ || captured_trees_ != d_trees || captured_status_ != d_status) {
+    cudaError_t e = capture(d_trees, d_status);
+    if (e != cudaSuccess) return e;
+  }
+  BatchHeader h = {};
+  h.n_items = (int)items.size();
+  for (const BatchItem& it : items) {
+    h.total_queries += it.nq;
+    h.total_buckets += it.buckets;
+    h.total_units += it.units;
+  }
+  h.next_unit = 0;
+  char* st = static_cast<char*>(h_stage_);
+  std::memcpy(st, &h, sizeof(h));
+  const size_t o_items = align256(sizeof(BatchHeader));
+  if (!items.empty()) std::memcpy(st + o_items, items.data(), sizeof(BatchItem) * items.size());
+  cudaError_t e = cudaMemcpyAsync(d_header_, st, o_items + sizeof(BatchItem) * items.size(),
+                                  cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return e;
+  return cudaGraphLaunch(exec_, stream);
+}
+
+}  // namespace sbh

@@ -1,0 +1,105 @@
+// Batched evaluation: many requests (trees, kernels, methods, query counts) in
+// one persistent launch, captured as a CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "device_common.cuh"
+
+namespace sbh {
+
+// One request of a batch, as the device reads it.
+struct BatchItem {
+  int tree;                  // index into the engine's tree table
+  int dim;                   // the tree's dimension
+  int method;                // SBH_METHOD_*
+  int kernel;                // SBH_KERNEL_*
+  int samples;               // stochastic method
+  float beta;                // Barnes-Hut
+  int sort_bits;             // Morton bits per axis of the query bucketing (0: keep order)
+  KParams kp;
+  unsigned long long seed;   // stochastic method
+  const float* q;            // device SoA [dim][nq]
+  float* out;                // device [nq]
+  int* contribs;             // device [nq] or null
+  const float* self_mass;    // device [nq] or null: subtract each query's own source term
+  long long nq;
+  long long query_base;      // index of q[0] within its whole request (keys the sampler's
+                             // random streams when a request is split across batches)
+  long long sort_base;       // first position of this request in the batch order array
+  long long bucket_base;     // first bucket of this request
+  long long buckets;         // buckets of this request
+  long long unit_base;       // first work unit of this request
+  long long units;           // work units of this request
+  float box_lo[3], box_hi[3];  // Morton box (the tree's root AABB)
+};
+
+struct BatchHeader {
+  int n_items;
+  int pad;
+  long long total_queries;
+  long long total_buckets;
+  long long total_units;
+  unsigned long long next_unit;  // work counter of the persistent kernel
+};
+
+// Queries per work unit (one warp task): Barnes-Hut and brute force evaluate
+// 32 queries per task (a lane each); the sampler gives each query a warp.
+constexpr int kUnitQueriesWarp = 32;
+constexpr int kUnitQueriesSampler = 2;
+
+class BatchEngine {
+ public:
+  struct Limits {
+    int max_items = 4096;
+    long long max_queries = 1 << 20;   // sorted positions (sum of request sizes)
+    int max_tree_depth = 128;          // deepest tree the engine will see
+    int max_root_children = 512;       // widest root the engine will see
+  };
+
+  // Creates the engine on the current device; `trees` is a device table of
+  // `n_trees` trees that batches index.
+  BatchEngine(const Limits& lim, int sm_count);
+  ~BatchEngine();
+  BatchEngine(const BatchEngine&) = delete;
+  BatchEngine& operator=(const BatchEngine&) = delete;
+
+  // Fills item bookkeeping (sort/bucket/unit ranges, sort bits) for `items`
+  // in place and checks limits.  Returns an error string or "".
+  std::string plan(std::vector<BatchItem>& items, const std::vector<DevTree>& host_trees) const;
+  // Enqueues the batch on `stream` (items already planned): copies the item
+  // table and header from pinned staging, then launches the captured graph.
+  cudaError_t launch(const std::vector<BatchItem>& items, const DevTree* d_trees,
+                     int* d_status, cudaStream_t stream);
+
+  const Limits& limits() const { return lim_; }
+  size_t device_bytes() const { return dev_bytes_; }
+
+ private:
+  cudaError_t capture(const DevTree* d_trees, int* d_status);
+
+  Limits lim_;
+  int sm_count_;
+  int eval_blocks_ = 0;
+  size_t eval_smem_ = 0;
+  // device buffers
+  void* dev_ = nullptr;
+  size_t dev_bytes_ = 0;
+  BatchHeader* d_header_ = nullptr;
+  BatchItem* d_items_ = nullptr;
+  unsigned* d_keys_ = nullptr;
+  unsigned* d_hist_ = nullptr;
+  int* d_order_ = nullptr;
+  // pinned staging of header + items
+  void* h_stage_ = nullptr;
+  // captured pipeline
+  cudaGraphExec_t exec_ = nullptr;
+  const DevTree* captured_trees_ = nullptr;
+  int* captured_status_ = nullptr;
+};
+
+}  // namespace sbh

@@ -16,8 +16,8 @@
 //     loop (brute_force_gpu.h:52-60) at a ~1/BF_SUB of its cost per pair.
 #include <cooperative_groups.h>
 
-#include "device_common.cuh"
 #include "launch.h"
+#include "tasks.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -29,45 +29,6 @@ constexpr int BF_QPT = 4;
 constexpr int BF_TILE = 512;
 constexpr int BF_SUB = 64;
 constexpr int BF_QUERIES_PER_CTA = BF_THREADS * BF_QPT;
-
-// Fast-path kernel values: same functions as kernel_exact, evaluated with FMA
-// and the hardware reciprocal square root.
-template <int DIM, int K>
-__device__ __forceinline__ float kernel_fast(float4 s, float4 nr, float3 q, const KParams& kp) {
-  const float dx = s.x - q.x, dy = s.y - q.y, dz = DIM == 3 ? s.z - q.z : 0.f;
-  if (K == kPlummer) {
-    float r2 = fmaf(dx, dx, kp.eps2);
-    r2 = fmaf(dy, dy, r2);
-    if (DIM == 3) r2 = fmaf(dz, dz, r2);
-    return s.w * rsqrtf(r2);
-  }
-  float r2 = dx * dx;
-  r2 = fmaf(dy, dy, r2);
-  if (DIM == 3) r2 = fmaf(dz, dz, r2);
-  if (K == kGravity) {
-    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
-    return __fdividef(-s.w, r + 1e-1f);
-  } else if (K == kWindingNumber) {
-    float qdn = nr.x * dx;
-    qdn = fmaf(nr.y, dy, qdn);
-    if (DIM == 3) qdn = fmaf(nr.z, dz, qdn);
-    if (DIM == 2) return __fdividef(s.w * qdn, kTwoPi * (r2 + 1e-5f));
-    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
-    return __fdividef(s.w * qdn, kFourPi * fmaf(r2, r, 1e-5f));
-  } else {  // smooth distance
-    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
-    return expf(-kp.alpha * r);
-  }
-}
-
-// Knuth two-sum of (hi, lo) += s.
-__device__ __forceinline__ void two_sum_add(float& hi, float& lo, float s) {
-  const float t = hi + s;
-  const float bp = t - hi;
-  const float e = (hi - (t - bp)) + (s - bp);
-  hi = t;
-  lo += e;
-}
 
 template <int DIM, int K>
 __global__ void __launch_bounds__(BF_THREADS) brute_force_kernel(DevTree t,

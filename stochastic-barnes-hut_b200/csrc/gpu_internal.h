@@ -1,0 +1,65 @@
+// Internals shared by the device-side C ABI files (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+struct sbh_gpu_tree {
+  int device = 0;
+  int sm_count = 0;
+  sbh::DevTree dev = {};
+  float box_lo[3] = {0, 0, 0}, box_hi[3] = {0, 0, 0};  // root AABB
+  void* mem = nullptr;  // one allocation: status word, points, nodes
+  size_t bytes = 0;
+  int* d_status = nullptr;
+  sbh_tree_info info = {};
+  std::mutex mu;        // serialises blocking calls (they share `ws`)
+  void* ws = nullptr;   // workspace of blocking calls
+  size_t ws_bytes = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace sbh {
+
+// Makes `dev` current for the scope and restores the previous device.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// Records a CUDA failure as the thread's error and returns its status.
+inline int cuda_fail(cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a sticky launch error so later calls are not poisoned
+  return fail(e == cudaErrorMemoryAllocation ? SBH_ERR_OUT_OF_MEMORY : SBH_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Validates an evaluation request against a tree; records the error.
+inline int check_eval_params(const sbh_gpu_tree* tree, const sbh_params* p, int64_t nq) {
+  if (!tree || !p) return fail(SBH_ERR_INVALID_ARGUMENT, "null tree or params");
+  if (nq < 0 || nq > (int64_t)INT32_MAX)
+    return fail(SBH_ERR_INVALID_ARGUMENT, "query count must be in [0, 2^31)");
+  if (p->method < SBH_METHOD_BRUTE_FORCE || p->method > SBH_METHOD_STOCHASTIC)
+    return fail(SBH_ERR_INVALID_ARGUMENT, "unknown method");
+  if (p->kernel < SBH_KERNEL_GRAVITY || p->kernel > SBH_KERNEL_PLUMMER)
+    return fail(SBH_ERR_INVALID_ARGUMENT, "unknown kernel");
+  if (p->method == SBH_METHOD_STOCHASTIC && p->samples_per_subdomain < 1)
+    return fail(SBH_ERR_INVALID_ARGUMENT, "samples_per_subdomain must be >= 1");
+  if (p->method == SBH_METHOD_STOCHASTIC &&
+      (int64_t)tree->info.root_children * p->samples_per_subdomain > (int64_t)INT32_MAX)
+    return fail(SBH_ERR_INVALID_ARGUMENT, "too many sampled paths per query");
+  return SBH_OK;
+}
+
+}  // namespace sbh

@@ -8,41 +8,13 @@
 #include <string>
 #include <vector>
 
-#include "internal.h"
+#include "gpu_internal.h"
 #include "launch.h"
-
-struct sbh_gpu_tree {
-  int device = 0;
-  int sm_count = 0;
-  sbh::DevTree dev = {};
-  void* mem = nullptr;  // one allocation: status word, points, nodes
-  size_t bytes = 0;
-  int* d_status = nullptr;
-  sbh_tree_info info = {};
-  std::mutex mu;        // serialises blocking calls (they share `ws`)
-  void* ws = nullptr;   // workspace of blocking calls
-  size_t ws_bytes = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-};
 
 namespace {
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
-
-int cuda_fail(cudaError_t e, const char* what) {
-  cudaGetLastError();  // clear a sticky launch error so later calls are not poisoned
-  return sbh::fail(e == cudaErrorMemoryAllocation ? SBH_ERR_OUT_OF_MEMORY : SBH_ERR_CUDA,
-                   std::string(what) + ": " + cudaGetErrorString(e));
-}
+using sbh::cuda_fail;
+using sbh::DeviceGuard;
 
 #define SBH_CK(call, what)                          \
   do {                                              \
@@ -51,22 +23,6 @@ int cuda_fail(cudaError_t e, const char* what) {
   } while (0)
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-
-int check_params(const sbh_gpu_tree* tree, const sbh_params* p, int64_t nq) {
-  if (!tree || !p) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null tree or params");
-  if (nq < 0 || nq > (int64_t)INT32_MAX)
-    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "query count must be in [0, 2^31)");
-  if (p->method < SBH_METHOD_BRUTE_FORCE || p->method > SBH_METHOD_STOCHASTIC)
-    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "unknown method");
-  if (p->kernel < SBH_KERNEL_GRAVITY || p->kernel > SBH_KERNEL_PLUMMER)
-    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "unknown kernel");
-  if (p->method == SBH_METHOD_STOCHASTIC && p->samples_per_subdomain < 1)
-    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "samples_per_subdomain must be >= 1");
-  if (p->method == SBH_METHOD_STOCHASTIC &&
-      (int64_t)tree->info.root_children * p->samples_per_subdomain > (int64_t)INT32_MAX)
-    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "too many sampled paths per query");
-  return SBH_OK;
-}
 
 // Device bytes an evaluation needs besides queries and results: the query
 // order and the sort workspace (0 when the method keeps the given order).
@@ -225,6 +181,10 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
   t.depth = h.depth;
   t.root_children = (nn > 0 && !h.leaf[0]) ? h.nch[0] : 0;
   t.alpha = h.alpha;
+  for (int k = 0; k < d; k++) {
+    g->box_lo[k] = h.bmin[k];
+    g->box_hi[k] = h.bmax[k];
+  }
   sbh::fill_info(h, &g->info);
   g->info.device_bytes = off;
   *out = g;
@@ -253,7 +213,7 @@ SBH_API int sbh_gpu_tree_info(const sbh_gpu_tree* tree, sbh_tree_info* info) {
 SBH_API int sbh_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* queries,
                      int64_t nq, float* results, int32_t* contribs, float* kernel_ms,
                      void* stream_ptr) {
-  int st = check_params(tree, params, nq);
+  int st = sbh::check_eval_params(tree, params, nq);
   if (st != SBH_OK) return st;
   if (nq > 0 && (!queries || !results))
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
@@ -309,7 +269,7 @@ SBH_API int sbh_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* 
 
 SBH_API int sbh_eval_device(sbh_gpu_tree* tree, const sbh_params* params, const float* d_queries,
                             int64_t nq, float* d_results, int32_t* d_contribs, void* stream_ptr) {
-  int st = check_params(tree, params, nq);
+  int st = sbh::check_eval_params(tree, params, nq);
   if (st != SBH_OK) return st;
   if (nq == 0) return sbh::ok();
   if (!d_queries || !d_results)
@@ -389,7 +349,7 @@ SBH_API int sbh_eval_device_static_scratch(sbh_gpu_tree* tree, const sbh_params*
                                            const float* d_queries, int64_t nq,
                                            float* d_results, int32_t* d_contribs,
                                            void* stream_ptr) {
-  int st = check_params(tree, params, nq);
+  int st = sbh::check_eval_params(tree, params, nq);
   if (st != SBH_OK) return st;
   if (nq > (int64_t)SBH_STATIC_SCRATCH_MAX_QUERIES)
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT,

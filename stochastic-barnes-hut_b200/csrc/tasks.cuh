@@ -1,0 +1,480 @@
+// Per-warp and per-query device routines shared by the single-call kernels
+// (barnes_hut.cu, sampler.cu, brute_force.cu) and the batched persistent kernel
+// (batch.cu).
+#pragma once
+
+#include "device_common.cuh"
+
+namespace sbh {
+
+// ============================================================ Barnes-Hut ===
+
+struct BhStackEntry {
+  int cur;        // next sibling to visit
+  int end;        // one past the last sibling
+  unsigned mask;  // lanes that visit this sibling range
+};
+
+// Kernel value of a query's own source (mass m at the query point): the term a
+// caller excludes when the queries are the sources themselves.
+template <int DIM, int K>
+__device__ __forceinline__ float self_term(float3 q, float m, const KParams& kp) {
+  return kernel_exact<DIM, K>(make_float4(q.x, q.y, q.z, m), make_float4(0.f, 0.f, 0.f, 0.f), q,
+                              kp);
+}
+
+// One warp evaluates the queries at sorted positions [slot0, slot_end) (at
+// most 32, one per lane) by a single depth-first walk of the union of the
+// lanes' opened sets.  The walk keeps, per tree level, a range of sibling nodes
+// still to visit and the mask of lanes that reach them (`stk`, stack_cap >=
+// tree depth + 2 entries).  At each node every lane in the mask applies the
+// reference's opening test (farFieldRatio >= beta, include/tree3d.h:134-153)
+// itself; lanes that accept add the node's aggregate (or its leaf points), the
+// others are passed on to the children.  So every lane visits exactly the nodes
+// evaluateBarnesHut_stackless (include/barnes_hut.h:23-78) visits for its query,
+// in the same depth-first, cell order, and adds the same FP32 values in the same
+// order: results and contribution counts equal the reference CPU's bit for bit.
+// With VOTE the lanes accept a node only if all of them do, which is the
+// reference GPU kernel's __all_sync semantics (include/barnes_hut_gpu.h:34).
+// self_mass (optional, indexed like the queries) subtracts each query's own
+// source term.
+template <int DIM, int K, bool VOTE>
+__device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __restrict__ qsoa,
+                                             long long nq, const int* __restrict__ order,
+                                             long long slot0, long long slot_end, float beta,
+                                             const KParams& kp, float* __restrict__ out,
+                                             int* __restrict__ contribs, int* status,
+                                             BhStackEntry* stk, int stack_cap,
+                                             const float* __restrict__ self_mass) {
+  const int lane = threadIdx.x & 31;
+  const long long slot = slot0 + lane;
+  const bool valid = slot < slot_end;
+  const unsigned active = __ballot_sync(0xffffffffu, valid);
+  if (active == 0) return;
+  const long long qi = valid ? (order ? (long long)__ldg(order + slot) : slot) : 0;
+  const float3 q = valid ? load_query<DIM>(qsoa, nq, qi) : make_float3(0.f, 0.f, 0.f);
+
+  float total = 0.f;
+  int nc = 0;
+  if (lane == 0) stk[0] = BhStackEntry{0, 1, active};
+  __syncwarp();
+  int sp = 1;
+  long long budget = t.nn + 1;  // a walk visits each node at most once
+  while (sp > 0) {
+    if (--budget < 0) {
+      if (lane == 0) report_status(status, kStatusTraversalLimit);
+      break;
+    }
+    const BhStackEntry e = stk[sp - 1];
+    __syncwarp();
+    const int node = e.cur;
+    if (e.cur + 1 == e.end) {
+      sp--;
+    } else if (lane == 0) {
+      stk[sp - 1].cur = e.cur + 1;
+    }
+    const bool in = (e.mask >> lane) & 1u;
+    // Topology and node record in one round trip (a one-point leaf's record is
+    // its point).
+    const int4 topo = __ldg(t.nd_topo + node);
+    const float4 cm = __ldg(t.nd_cm + node);
+    const bool leaf = topo.y == 0;
+    bool acc = false;
+    if (leaf) {
+      acc = in && (__int_as_float(0x7f800000) >= beta);
+    } else if (in) {
+      acc = far_field_ratio<DIM>(cm, q) >= beta;
+    }
+    if (VOTE) {
+      const unsigned rej = __ballot_sync(0xffffffffu, in && !acc);
+      acc = in && rej == 0u;
+    }
+    if (acc) {
+      if (leaf && topo.w - topo.z != 1) {
+        for (int i = topo.z; i < topo.w; i++) {
+          total = radd(total, kernel_exact<DIM, K>(__ldg(t.pt_pm + i), __ldg(t.pt_nrm + i), q, kp));
+          nc++;
+        }
+      } else {
+        total = radd(total, kernel_node<DIM, K>(cm, __ldg(t.nd_agg + node), q, kp));
+        nc++;
+      }
+    }
+    const unsigned open = __ballot_sync(0xffffffffu, in && !acc);
+    if (open != 0u && !leaf) {
+      if (sp >= stack_cap) {
+        if (lane == 0) report_status(status, kStatusStackOverflow);
+        break;
+      }
+      if (lane == 0) stk[sp] = BhStackEntry{topo.x, topo.x + topo.y, open};
+      sp++;
+    }
+    __syncwarp();
+  }
+  if (valid) {
+    if (self_mass) total = rsub(total, self_term<DIM, K>(q, __ldg(self_mass + qi), kp));
+    out[qi] = total;
+    if (contribs) contribs[qi] = nc;
+  }
+}
+
+// ============================================================ sampler ===
+
+constexpr int SBH_VCAP = 512;  // node/child values buffered per warp per pass
+
+// Per-warp shared-memory scratch of the expansion step.
+struct ExpandSmem {
+  float* vals;      // [SBH_VCAP] node and child values of the current pass
+  int* ent;         // [SBH_VCAP] node evaluated at each entry of the current pass
+  unsigned* multi;  // [SBH_VCAP/32] entries that are leaves with several points
+};
+
+// acc += k(point) for every point of leaf tc, in order (rare: leaves with
+// several points exist only for leaf sizes > 1 or at the depth cap).
+template <int DIM, int K>
+__device__ __forceinline__ float add_leaf_points(const DevTree& t, int4 tc, float3 q,
+                                                 const KParams& kp, float acc) {
+  for (int i = tc.z; i < tc.w; i++)
+    acc = radd(acc, kernel_exact<DIM, K>(__ldg(t.pt_pm + i), __ldg(t.pt_nrm + i), q, kp));
+  return acc;
+}
+
+// Expansion of up to 32 internal nodes at once.  Lane l owns node `v` (topo tv)
+// when `own`.  The warp evaluates, as one flat list, every owner's node followed
+// by its children (each owner writes its own entries' node indices, then all
+// lanes evaluate 32 consecutive entries at a time); the owner gets back
+// kv = k(v) and the children sum sum_{children c} k(c) in cell order, leaf
+// children point by point (include/tree_sampler.h:264-280), and `contribs`, the
+// number of kernel evaluations that sum stands for.  All lanes must call.
+template <int DIM, int K>
+__device__ __forceinline__ float expand(const DevTree& t, bool own, int v, int4 tv, float3 q,
+                                        const KParams& kp, const ExpandSmem& sm, int lane,
+                                        float& kv, int& contribs) {
+  const int nent = own ? tv.y + 1 : 0;
+  int incl = nent;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int excl = incl - nent;
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  float acc = 0.f;
+  kv = 0.f;
+  contribs = 0;
+  for (int base = 0; base < total; base += SBH_VCAP) {
+    const int end = min(total, base + SBH_VCAP);
+    const int s0 = max(excl, base), s1 = min(excl + nent, end);
+    for (int p = s0; p < s1; p++) sm.ent[p - base] = p == excl ? v : tv.x + (p - excl - 1);
+    if (lane < SBH_VCAP / 32) sm.multi[lane] = 0u;
+    __syncwarp();
+    for (int r = lane; r < end - base; r += 32) {
+      // Node record: an aggregate, or for a one-point leaf the point itself.
+      const int c = sm.ent[r];
+      const int4 tc = __ldg(t.nd_topo + c);
+      const float4 cm = __ldg(t.nd_cm + c), ag = __ldg(t.nd_agg + c);
+      if (tc.y == 0 && tc.w - tc.z != 1) atomicOr(sm.multi + (r >> 5), 1u << (r & 31));
+      sm.vals[r] = kernel_node<DIM, K>(cm, ag, q, kp);
+    }
+    __syncwarp();
+    for (int p = s0; p < s1; p++) {
+      const int r = p - base;
+      if (p == excl) {
+        kv = sm.vals[r];
+      } else if ((sm.multi[r >> 5] >> (r & 31)) & 1u) {
+        const int4 tc = __ldg(t.nd_topo + tv.x + (p - excl - 1));
+        acc = add_leaf_points<DIM, K>(t, tc, q, kp, acc);
+        contribs += tc.w - tc.z;
+      } else {
+        acc = radd(acc, sm.vals[r]);
+        contribs += 1;
+      }
+    }
+    __syncwarp();
+  }
+  return acc;
+}
+
+// containedInChild(VectorNd p) (include/tree3d.h:172-183): the child of v whose
+// cell holds p, skipping single-child chains.  A cell without a child reads the
+// root (child_buffer_idxs_ is value-initialised to 0 in the reference).
+// Returns -1 where the reference would return nullptr.
+template <int DIM>
+__device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 tv, float3 p,
+                                                  int4& tout) {
+  for (int guard = 0; guard <= t.depth + 1; guard++) {
+    const float4 lo = __ldg(t.nd_bmin + v), hi = __ldg(t.nd_bmax + v);
+    if (!aabb_contains<DIM>(lo, hi, p)) return -1;
+    const int cx = quantize1(p.x, lo.x, hi.x, t.ds);
+    const int cy = quantize1(p.y, lo.y, hi.y, t.ds);
+    const int cz = DIM == 3 ? quantize1(p.z, lo.z, hi.z, t.ds) : 0;
+    const int cell = (((cz << t.dsl) + cy) << t.dsl) + cx;
+    const unsigned long long* m = t.nd_mask + (long long)v * t.mw;
+    const int w = cell >> 6, b = cell & 63;
+    const unsigned long long word = __ldg(m + w);
+    int child = 0;
+    if ((word >> b) & 1ull) {
+      int rank = __popcll(word & ((1ull << b) - 1ull));
+      for (int k = 0; k < w; k++) rank += __popcll(__ldg(m + k));
+      child = tv.x + rank;
+    }
+    const int4 tc = __ldg(t.nd_topo + child);
+    if (tc.y != 1) {
+      tout = tc;
+      return child;
+    }
+    v = child;
+    tv = tc;
+  }
+  return -1;
+}
+
+
+// Shared-memory scratch of one warp running the sampler (sbh_warp_words floats).
+struct SbhWarpSmem {
+  float* bhS;     // [R] BH term of each subdomain
+  float* diffS;   // [R] first-step difference of each subdomain
+  int* ccS;       // [R] contributions of that difference
+  float* pathv;   // [32] per-path corrections of the current round
+  ExpandSmem ex;
+};
+
+__host__ __device__ constexpr int sbh_warp_words(int R) {
+  return 3 * R + 32 + 2 * SBH_VCAP + SBH_VCAP / 32;
+}
+
+__device__ __forceinline__ SbhWarpSmem sbh_carve(float* base, int R) {
+  SbhWarpSmem w;
+  w.bhS = base;
+  w.diffS = base + R;
+  w.ccS = reinterpret_cast<int*>(base + 2 * R);
+  w.pathv = base + 3 * R;
+  w.ex.vals = w.pathv + 32;
+  w.ex.ent = reinterpret_cast<int*>(w.ex.vals + SBH_VCAP);
+  w.ex.multi = reinterpret_cast<unsigned*>(w.ex.ent + SBH_VCAP);
+  return w;
+}
+
+// The whole estimator for one query, one warp: see sampler.cu for the method.
+// qi is the query's index in its request (it keys the Philox streams).  The
+// result and its contribution count are returned on lane 0.
+template <int DIM, int K>
+__device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long qi, int samples,
+                                          unsigned long long seed, const KParams& kp,
+                                          const SbhWarpSmem& ws, int* status, float& result,
+                                          int& count) {
+  const int lane = threadIdx.x & 31;
+  const int R = t.root_children;
+  const float inf = __int_as_float(0x7f800000);
+  const int c0 = __ldg(t.nd_topo).x;
+  result = 0.f;
+  count = 0;
+  if (R == 0) return;  // a single-leaf tree has no subdomains (tree_sampler.h:214)
+  int cnt = 0;
+
+  // Phase A: BH term and first-step difference of every subdomain.
+  for (int g = 0; g < R; g += 32) {
+    const int j = g + lane;
+    const bool have = j < R;
+    int4 tS = make_int4(0, 0, 0, 0);
+    if (have) {
+      tS = __ldg(t.nd_topo + c0 + j);
+      // a leaf subdomain's points are added in order by lane 0 below
+      cnt += tS.y != 0 ? 1 : tS.w - tS.z;
+    }
+    const bool own = have && tS.y != 0;
+    int cc;
+    float kS;
+    const float sumc = expand<DIM, K>(t, own, c0 + j, tS, q, kp, ws.ex, lane, kS, cc);
+    if (have) {
+      ws.bhS[j] = kS;
+      ws.diffS[j] = own ? rsub(sumc, kS) : 0.f;
+      ws.ccS[j] = cc;
+    }
+  }
+  __syncwarp();
+
+  // Phase B: sampled paths, 32 at a time, advanced step by step in lock step.
+  const int P = R * samples;
+  float mlcv = 0.f, sub = 0.f;
+  int cur_sub = -1;
+  for (int pbase = 0; pbase < P; pbase += 32) {
+    const int pid = pbase + lane;
+    float wd = 0.f;
+    bool active = false;
+    int j = 0, S = 0, cur = 0;
+    int4 tcur = make_int4(0, 0, 0, 0);
+    float spi = 0.f, ev = 1.f, cb = 1.f;
+    float3 p = make_float3(0.f, 0.f, 0.f);
+    PathRng rng;
+    if (pid < P) {
+      j = pid / samples;
+      S = c0 + j;
+      const int4 tS = __ldg(t.nd_topo + S);
+      rng.begin(seed, (unsigned long long)qi, (uint32_t)pid);
+      const uint32_t nS = (uint32_t)(tS.w - tS.z);
+      const int idx = tS.z + (int)rng.index(nS);
+      const float4 sp = __ldg(t.pt_pm + idx);
+      p = make_float3(sp.x, sp.y, sp.z);
+      spi = (float)nS;
+      cur = S;
+      tcur = tS;
+      const float r0 = tS.y == 0 ? inf : far_field_ratio<DIM>(__ldg(t.nd_cm + S), q);
+      cb = (1.f < r0) ? r0 : 1.f;
+      active = tS.y != 0;
+    }
+    while (__any_sync(0xffffffffu, active)) {
+      bool own = false;
+      int prev = 0;
+      int4 tprev = make_int4(0, 0, 0, 0);
+      float w = 0.f;
+      if (active) {
+        const float4 cmc = __ldg(t.nd_cm + cur);
+        const float ffr = far_field_ratio<DIM>(cmc, q);
+        const float ratio = rdiv(cb, ffr);
+        const float tp = (1.f < ratio) ? 1.f : ratio;
+        const float u = rng.uniform();
+        if (u > tp) {
+          active = false;
+        } else {
+          ev = rmul(ev, tp);
+          prev = cur;
+          tprev = tcur;
+          int4 tnext;
+          cur = contained_in_child<DIM>(t, prev, tprev, p, tnext);
+          if (cur < 0) {
+            report_status(status, kStatusNullChild);
+            wd = __int_as_float(0x7fc00000);
+            active = false;
+          } else {
+            cb = (cb < ffr) ? ffr : cb;
+            w = rdiv(spi, rmul(ev, (float)(unsigned)(tprev.w - tprev.z)));
+            if (prev == S) {
+              wd = radd(wd, rmul(w, ws.diffS[j]));
+              cnt += ws.ccS[j];
+            } else {
+              own = true;
+            }
+            tcur = tnext;
+            if (tcur.y == 0) active = false;
+          }
+        }
+      }
+      int cc;
+      float kprev;
+      const float sumc = expand<DIM, K>(t, own, prev, tprev, q, kp, ws.ex, lane, kprev, cc);
+      if (own) {
+        wd = radd(wd, rmul(w, rsub(sumc, kprev)));
+        cnt += cc;
+      }
+    }
+    ws.pathv[lane] = wd;
+    __syncwarp();
+    if (lane == 0) {
+      const int m = min(32, P - pbase);
+      for (int k = 0; k < m; k++) {
+        const int jj = (pbase + k) / samples;
+        if (jj != cur_sub) {
+          if (cur_sub >= 0) mlcv = radd(mlcv, rdiv(sub, (float)samples));
+          sub = 0.f;
+          cur_sub = jj;
+        }
+        sub = radd(sub, ws.pathv[k]);
+      }
+    }
+    __syncwarp();
+  }
+
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0) {
+    if (cur_sub >= 0) mlcv = radd(mlcv, rdiv(sub, (float)samples));
+    float bh = 0.f;
+    for (int j = 0; j < R; j++) {
+      const int4 tS = __ldg(t.nd_topo + c0 + j);
+      if (tS.y == 0) {
+        bh = add_leaf_points<DIM, K>(t, tS, q, kp, bh);
+      } else {
+        bh = radd(bh, ws.bhS[j]);
+      }
+    }
+    result = radd(bh, mlcv);
+    count = cnt;
+  }
+  __syncwarp();  // the next query of this warp overwrites the scratch
+}
+
+// ======================================================= brute force ===
+
+// Fast-path kernel values: same functions as kernel_exact, evaluated with FMA
+// and the hardware reciprocal square root (brute force only).
+template <int DIM, int K>
+__device__ __forceinline__ float kernel_fast(float4 s, float4 nr, float3 q, const KParams& kp) {
+  const float dx = s.x - q.x, dy = s.y - q.y, dz = DIM == 3 ? s.z - q.z : 0.f;
+  if (K == kPlummer) {
+    float r2 = fmaf(dx, dx, kp.eps2);
+    r2 = fmaf(dy, dy, r2);
+    if (DIM == 3) r2 = fmaf(dz, dz, r2);
+    return s.w * rsqrtf(r2);
+  }
+  float r2 = dx * dx;
+  r2 = fmaf(dy, dy, r2);
+  if (DIM == 3) r2 = fmaf(dz, dz, r2);
+  if (K == kGravity) {
+    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+    return __fdividef(-s.w, r + 1e-1f);
+  } else if (K == kWindingNumber) {
+    float qdn = nr.x * dx;
+    qdn = fmaf(nr.y, dy, qdn);
+    if (DIM == 3) qdn = fmaf(nr.z, dz, qdn);
+    if (DIM == 2) return __fdividef(s.w * qdn, kTwoPi * (r2 + 1e-5f));
+    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+    return __fdividef(s.w * qdn, kFourPi * fmaf(r2, r, 1e-5f));
+  } else {  // smooth distance
+    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+    return expf(-kp.alpha * r);
+  }
+}
+
+// Knuth two-sum of (hi, lo) += s.
+__device__ __forceinline__ void two_sum_add(float& hi, float& lo, float s) {
+  const float t = hi + s;
+  const float bp = t - hi;
+  const float e = (hi - (t - bp)) + (s - bp);
+  hi = t;
+  lo += e;
+}
+
+// Brute force for one warp of queries (lane per query, sources read as warp
+// broadcasts): the batched path's brute-force task.  Plain FP32 sums over 64
+// sources, merged by two-sum, as brute_force.cu does.
+template <int DIM, int K>
+__device__ __forceinline__ void bf_warp_task(const DevTree& t, const float* __restrict__ qsoa,
+                                             long long nq, long long slot0, long long slot_end,
+                                             const KParams& kp, float* __restrict__ out,
+                                             int* __restrict__ contribs,
+                                             const float* __restrict__ self_mass) {
+  const int lane = threadIdx.x & 31;
+  const long long qi = slot0 + lane;
+  const bool valid = qi < slot_end;
+  const float3 q = valid ? load_query<DIM>(qsoa, nq, qi) : make_float3(0.f, 0.f, 0.f);
+  float hi = 0.f, lo = 0.f;
+  for (long long b = 0; b < t.n; b += 64) {
+    const long long e = min(t.n, b + 64);
+    float part = 0.f;
+    for (long long i = b; i < e; i++) {
+      const float4 s = __ldg(t.pt_pm + i);
+      const float4 nr = K == kWindingNumber ? __ldg(t.pt_nrm + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+      part += kernel_fast<DIM, K>(s, nr, q, kp);
+    }
+    two_sum_add(hi, lo, part);
+  }
+  if (valid) {
+    float v = hi + lo;
+    if (self_mass) v -= self_term<DIM, K>(q, __ldg(self_mass + qi), kp);
+    out[qi] = v;
+    if (contribs) contribs[qi] = (int)t.n;
+  }
+}
+
+}  // namespace sbh

@@ -53,6 +53,14 @@ _SIGNATURES = {
     "sbh_eval_device": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
     "sbh_gpu_tree_check": (ctypes.c_int, [_P, _P]),
     "sbh_eval_device_static_scratch": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
+    "sbh_eval_batch": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+    "sbh_server_config_init": (None, [_P]),
+    "sbh_server_create": (ctypes.c_int, [_P, _P]),
+    "sbh_server_add_tree": (ctypes.c_int, [_P, _P, _P]),
+    "sbh_server_submit": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _I64, _P, _P, _P]),
+    "sbh_server_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_double, _P]),
+    "sbh_server_stats_get": (ctypes.c_int, [_P, _P]),
+    "sbh_server_destroy": (None, [_P]),
 }
 
 # Largest query count sbh_eval_device_static_scratch accepts per call.
@@ -73,6 +81,27 @@ class TreeInfo(ctypes.Structure):
                 ("depth", ctypes.c_int32), ("root_children", ctypes.c_int32),
                 ("alpha", ctypes.c_float), ("reserved", ctypes.c_int32),
                 ("device_bytes", ctypes.c_uint64)]
+
+
+class BatchItem(ctypes.Structure):
+    _fields_ = [("tree", _P), ("params", Params), ("d_queries", _P), ("nq", ctypes.c_int64),
+                ("d_results", _P), ("d_contribs", _P), ("d_self_mass", _P)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("slots", ctypes.c_int32),
+                ("slot_queries", ctypes.c_int64), ("max_requests_per_batch", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("batches", ctypes.c_int32), ("nq", ctypes.c_int64),
+                ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_int64), ("queries", ctypes.c_int64),
+                ("batches", ctypes.c_int64), ("busy_ms", ctypes.c_double)]
 
 
 class SbhError(RuntimeError):
@@ -234,6 +263,92 @@ class GpuTree:
     def close(self):
         if getattr(self, "handle", None) and _lib is not None:
             _lib.sbh_gpu_tree_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        self.close()
+
+
+def eval_batch(entries, stream: int = 0):
+    """sbh_eval_batch: entries are (gpu_tree, params, d_queries, nq, d_results,
+    d_contribs or 0, d_self_mass or 0) with device pointers; one pipeline for all."""
+    arr = (BatchItem * len(entries))()
+    for i, (tree, p, dq, nq, dout, dcnt, dself) in enumerate(entries):
+        arr[i].tree = tree.handle
+        arr[i].params = p
+        arr[i].d_queries = dq
+        arr[i].nq = nq
+        arr[i].d_results = dout
+        arr[i].d_contribs = dcnt or None
+        arr[i].d_self_mass = dself or None
+    _check(lib().sbh_eval_batch(arr, len(entries), ctypes.c_void_p(stream)))
+
+
+class Request:
+    """A request submitted to a Server; `results` fills in when wait() returns."""
+
+    def __init__(self, server, rid, queries, results, contribs):
+        self.server, self.id = server, rid
+        self._queries = queries  # kept alive until the request finishes
+        self.results, self.contribs = results, contribs
+        self.info = None
+
+    def wait(self, timeout_ms: float = -1.0):
+        if self.info is None:
+            info = RequestInfo()
+            _check(lib().sbh_server_wait(self.server.handle, self.id, timeout_ms,
+                                         ctypes.byref(info)))
+            self.info = {"status": info.status, "batches": info.batches, "nq": info.nq,
+                         "queue_ms": info.queue_ms, "latency_ms": info.latency_ms}
+            self._queries = None
+            if info.status != OK:
+                raise SbhError(info.status, "request failed")
+        return self.results
+
+
+class Server:
+    """sbh_server_*: resident trees and continuous batching on one device."""
+
+    def __init__(self, device=0, slots=3, slot_queries=1 << 20, max_requests_per_batch=4096):
+        cfg = ServerConfig()
+        lib().sbh_server_config_init(ctypes.byref(cfg))
+        cfg.device, cfg.slots, cfg.slot_queries = device, slots, slot_queries
+        cfg.max_requests_per_batch = max_requests_per_batch
+        h = ctypes.c_void_p()
+        _check(lib().sbh_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.handle = h
+        self.dims = []
+
+    def add_tree(self, host: HostTree) -> int:
+        tid = ctypes.c_int32()
+        _check(lib().sbh_server_add_tree(self.handle, host.handle, ctypes.byref(tid)))
+        self.dims.append(host.info().dim)
+        return tid.value
+
+    def submit(self, tree_id: int, queries, p: Params, contribs: bool = False) -> Request:
+        if not 0 <= tree_id < len(self.dims):
+            raise SbhError(ERR_INVALID_ARGUMENT, "unknown tree id")
+        dim = self.dims[tree_id]
+        q = np.asfortranarray(queries, np.float32)
+        if q.ndim != 2 or q.shape[1] != dim:
+            raise ValueError(f"queries must be (n, {dim})")
+        nq = q.shape[0]
+        out = np.empty(nq, np.float32)
+        cnt = np.empty(nq, np.int32) if contribs else None
+        rid = ctypes.c_uint64()
+        _check(lib().sbh_server_submit(self.handle, tree_id, ctypes.byref(p), _ptr(q), nq,
+                                       _ptr(out), _ptr(cnt), ctypes.byref(rid)))
+        return Request(self, rid.value, q, out, cnt)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().sbh_server_stats_get(self.handle, ctypes.byref(st)))
+        return {"requests": st.requests, "queries": st.queries, "batches": st.batches,
+                "busy_ms": st.busy_ms}
+
+    def close(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.sbh_server_destroy(self.handle)
         self.handle = None
 
     def __del__(self):

@@ -33,6 +33,9 @@ def test_ctypes_binding_covers_the_header():
 def test_struct_layouts():
     assert ctypes.sizeof(C.Params) == 40
     assert ctypes.sizeof(C.TreeInfo) == 56
+    assert ctypes.sizeof(C.BatchItem) == 88
+    assert ctypes.sizeof(C.ServerConfig) == 24
+    assert ctypes.sizeof(C.RequestInfo) == 32
     assert C.lib().sbh_abi_version() == 1
 
 

@@ -1,0 +1,161 @@
+"""Batched evaluation and the serving loop on the GPU.
+
+Every request's result must be the same in a batch or in the server's mix as
+when evaluated alone: bit for bit for Barnes-Hut and the sampler (per-query
+exact traversal; random streams keyed by (seed, query index in the request)),
+within the brute-force tolerance for brute force (the batch runs a different
+summation schedule)."""
+import threading
+
+import numpy as np
+import pytest
+
+import sbh_capi as C
+import sbh_workloads as W
+from helpers import bits_equal
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    torch = pytest.importorskip("torch")
+    trees = {}
+    pts, nrm, a = W.torus_surface(30000, seed=91)
+    lo, hi = W.padded_box(pts)
+    trees["torus2"] = C.HostTree(pts, nrm, a, lo, hi, dim_split_log=2)
+    pts, nrm, m = W.gaussian_mixture(20000, seed=92)
+    lo, hi = W.padded_box(pts)
+    trees["gauss1"] = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=1)
+    trees["gauss1_pts"] = (pts, m)
+    pts, nrm, m = W.circle_points(20000, seed=93)
+    lo, hi = W.padded_box(pts)
+    trees["circle2"] = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=2, alpha=30.0)
+    gpus = {k: C.GpuTree(v) for k, v in trees.items() if isinstance(v, C.HostTree)}
+    return torch, trees, gpus
+
+
+def _dev(torch, q):
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(q, np.float32).T)).cuda()
+
+
+REQUESTS = [
+    # tree, method, kernel, nq, extra params
+    ("torus2", C.STOCHASTIC, C.WINDING_NUMBER, 1000, dict(samples_per_subdomain=2, seed=5)),
+    ("torus2", C.BARNES_HUT, C.WINDING_NUMBER, 33, dict(beta=2.0)),
+    ("gauss1", C.BARNES_HUT, C.GRAVITY, 5000, dict(beta=1.25)),
+    ("gauss1", C.STOCHASTIC, C.PLUMMER, 1, dict(samples_per_subdomain=3, seed=9)),
+    ("circle2", C.STOCHASTIC, C.SMOOTH_DIST, 700, dict(samples_per_subdomain=1, seed=1)),
+    ("circle2", C.BARNES_HUT_VOTE, C.GRAVITY, 300, dict(beta=2.0)),
+    ("gauss1", C.BRUTE_FORCE, C.GRAVITY, 100, dict()),
+    ("torus2", C.STOCHASTIC, C.GRAVITY, 2000, dict(samples_per_subdomain=1, seed=2,
+                                                   flags=C.FLAG_KEEP_ORDER)),
+    ("gauss1", C.BARNES_HUT, C.PLUMMER, 0, dict(beta=2.0)),
+]
+
+
+def _check_same(method, kernel, got, want):
+    if method == C.BRUTE_FORCE:
+        assert np.allclose(got, want, rtol=2e-6, atol=0)
+    elif kernel == C.SMOOTH_DIST:
+        assert np.allclose(got, want, rtol=1e-5, atol=1e-30)
+    else:
+        assert bits_equal(got, want)
+
+
+def test_batch_matches_single_calls(env):
+    torch, trees, gpus = env
+    rng = np.random.default_rng(94)
+    entries, checks = [], []
+    for name, method, kernel, nq, extra in REQUESTS:
+        dim = gpus[name].dim
+        q = rng.uniform(-1.2, 1.2, (nq, dim)).astype(np.float32)
+        p = C.params(method=method, kernel=kernel, **extra)
+        dq = _dev(torch, q) if nq else torch.empty((dim, 1), device="cuda")
+        out = torch.empty(max(nq, 1), dtype=torch.float32, device="cuda")
+        cnt = torch.empty(max(nq, 1), dtype=torch.int32, device="cuda")
+        entries.append((gpus[name], p, dq.data_ptr(), nq, out.data_ptr(), cnt.data_ptr(), 0))
+        checks.append((name, method, kernel, q, p, dq, out, cnt))
+    stream = torch.cuda.current_stream().cuda_stream
+    C.eval_batch(entries, stream=stream)
+    # A second batch on the same engine (reuses the captured graph).
+    C.eval_batch(entries[::-1], stream=stream)
+    torch.cuda.synchronize()
+    for name, method, kernel, q, p, dq, out, cnt in checks:
+        if len(q) == 0:
+            continue
+        want, _, wcnt = gpus[name].eval(q, p, contribs=True)
+        _check_same(method, kernel, out.cpu().numpy()[:len(q)], want)
+        if method != C.BRUTE_FORCE:
+            assert np.array_equal(cnt.cpu().numpy()[:len(q)], wcnt)
+
+
+def test_batch_excludes_self_terms(env):
+    torch, trees, gpus = env
+    pts, m = trees["gauss1_pts"]
+    q = pts[:3000]
+    p = C.params(method=C.BARNES_HUT, kernel=C.GRAVITY, beta=2.0)
+    dq = _dev(torch, q)
+    dm = torch.from_numpy(m[:3000]).cuda()
+    out = torch.empty(3000, dtype=torch.float32, device="cuda")
+    C.eval_batch([(gpus["gauss1"], p, dq.data_ptr(), 3000, out.data_ptr(), 0, dm.data_ptr())],
+                 stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    full, _ = gpus["gauss1"].eval(q, p)
+    self_term = np.float32(-1.0) * m[:3000] / np.float32(0.1)  # -m / (0 + 0.1), IEEE float32
+    assert bits_equal(out.cpu().numpy(), (full - self_term).astype(np.float32))
+
+
+def test_server_same_alone_and_in_the_mix(env):
+    torch, trees, gpus = env
+    # Small slots force requests to be split across batches.
+    server = C.Server(slots=3, slot_queries=4096, max_requests_per_batch=64)
+    ids = {name: server.add_tree(trees[name]) for name in ("torus2", "gauss1", "circle2")}
+    rng = np.random.default_rng(95)
+    jobs = []
+    for i in range(60):
+        name, method, kernel, _, extra = REQUESTS[i % 8]
+        nq = int(rng.integers(1, 9000))
+        dim = gpus[name].dim
+        q = rng.uniform(-1.2, 1.2, (nq, dim)).astype(np.float32)
+        jobs.append((name, C.params(method=method, kernel=kernel, **extra), q))
+    results = [None] * len(jobs)
+
+    def worker(k):
+        reqs = [(j, server.submit(ids[jobs[j][0]], jobs[j][2], jobs[j][1], contribs=True))
+                for j in range(k, len(jobs), 4)]
+        for j, r in reqs:
+            r.wait()
+            results[j] = r
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    split = 0
+    for (name, p, q), r in zip(jobs, results):
+        want, _, wcnt = gpus[name].eval(q, p, contribs=True)
+        _check_same(p.method, p.kernel, r.results, want)
+        if p.method != C.BRUTE_FORCE:
+            assert np.array_equal(r.contribs, wcnt)
+        assert r.info["status"] == C.OK and r.info["latency_ms"] >= r.info["queue_ms"] >= 0
+        split += r.info["batches"] > 1
+    assert split > 0
+    st = server.stats()
+    assert st["requests"] == len(jobs) and st["batches"] >= split
+    server.close()
+
+
+def test_server_rejects_bad_requests(env):
+    torch, trees, gpus = env
+    server = C.Server(slots=1, slot_queries=1024)
+    tid = server.add_tree(trees["gauss1"])
+    with pytest.raises(C.SbhError):
+        server.submit(tid + 5, np.zeros((4, 3), np.float32), C.params(method=C.BARNES_HUT))
+    with pytest.raises(C.SbhError):
+        server.submit(tid, np.zeros((4, 3), np.float32),
+                      C.params(method=C.STOCHASTIC, samples_per_subdomain=0))
+    r = server.submit(tid, np.zeros((0, 3), np.float32), C.params(method=C.BARNES_HUT))
+    assert r.wait().shape == (0,)
+    server.close()
