@@ -493,13 +493,271 @@ def run_reference(args, wl):
     }
 
 
+# ----------------------------------------------------------------- serving
+
+SERVING_KERNELS = ("gravity", "wn", "smooth")
+
+
+def serving_setup(C, seed=77, n_trees=32, n_requests=1500):
+    """32 resident trees (16 3D, 16 2D; Gaussian mixtures, torus, sphere and
+    circle surfaces; 10^4..2*10^6 points log-uniform) and a seeded request list:
+    tree, kernel (gravity / winding number / smooth distance alpha 100), query
+    count log-uniform in [1, 10^5] uniform in the tree's box, budget 64/256/1024."""
+    import sbh_workloads as W
+    rng = np.random.default_rng(seed)
+    trees = []
+    for i in range(n_trees):
+        dim = 3 if i < n_trees // 2 else 2
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        if dim == 3:
+            kind = ("gauss", "torus", "sphere")[i % 3]
+            pts, nrm, m = (W.gaussian_mixture(n, seed + i) if kind == "gauss" else
+                           W.torus_surface(n, seed + i) if kind == "torus" else
+                           W.sphere_surface(n, seed + i))
+        else:
+            kind = ("gauss", "circle")[i % 2]
+            pts, nrm, m = (W.gaussian_mixture(n, seed + i, dim=2) if kind == "gauss" else
+                           W.circle_points(n, seed + i))
+        lo, hi = W.padded_box(pts)
+        h1 = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=1)
+        h2 = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=2)
+        trees.append(dict(dim=dim, kind=kind, n=n, lo=lo, hi=hi, bh=h1, sbh=h2,
+                          root2=h2.info().root_children))
+    reqs = []
+    for r in range(n_requests):
+        ti = int(rng.integers(n_trees))
+        t = trees[ti]
+        kern = SERVING_KERNELS[int(rng.integers(3))]
+        nq = int(np.exp(rng.uniform(0.0, np.log(1e5))))
+        budget = int(rng.choice([64, 256, 1024]))
+        q = rng.uniform(t["lo"], t["hi"], (nq, t["dim"])).astype(np.float32)
+        reqs.append(dict(tree=ti, kernel=kern, nq=nq, budget=budget, q=np.asfortranarray(q)))
+    return trees, reqs
+
+
+def serving_params(C, W, t, r, method, theta=0.5):
+    kid = {"gravity": C.GRAVITY, "wn": C.WINDING_NUMBER, "smooth": C.SMOOTH_DIST}[r["kernel"]]
+    alpha = 100.0 if r["kernel"] == "smooth" else None
+    if method == "sbh":
+        return C.params(method=C.STOCHASTIC, kernel=kid, alpha=alpha, seed=r["nq"],
+                        samples_per_subdomain=W.samples_for_budget(r["budget"], t["root2"]))
+    return C.params(method=C.BARNES_HUT, kernel=kid, alpha=alpha, beta=1.0 / theta)
+
+
+def wait_until(t0, at):
+    while True:
+        d = at - (time.perf_counter() - t0)
+        if d <= 0:
+            return
+        time.sleep(d if d > 2e-3 else 0)
+
+
+def drive_plain(C, W, trees, reqs, gpus, arrivals, method="bh"):
+    """The reference's usage: one blocking call per request, in arrival order."""
+    outs = []
+    lat = []
+    t0 = time.perf_counter()
+    for r, at in zip(reqs, arrivals):
+        wait_until(t0, at)
+        t = trees[r["tree"]]
+        out = np.empty(r["nq"], np.float32)
+        g = gpus[r["tree"]]
+        g.eval_host_ptr(r["q"].ctypes.data, r["nq"], out.ctypes.data,
+                        serving_params(C, W, t, r, method))
+        lat.append((time.perf_counter() - t0 - at) * 1e3)
+        outs.append(out)
+    return time.perf_counter() - t0, np.array(lat), outs
+
+
+def drive_served(C, W, trees, reqs, server, ids, arrivals, method):
+    handles = [None] * len(reqs)
+    lateness = np.zeros(len(reqs))
+
+    def submitter():
+        t0s = t0
+        for k, (r, at) in enumerate(zip(reqs, arrivals)):
+            wait_until(t0s, at)
+            lateness[k] = (time.perf_counter() - t0s - at) * 1e3
+            t = trees[r["tree"]]
+            handles[k] = server.submit(ids[(r["tree"], method)], r["q"],
+                                       serving_params(C, W, t, r, method))
+
+    t0 = time.perf_counter()
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    lat = []
+    for k, h in enumerate(handles):
+        h.wait()
+        lat.append(h.info["latency_ms"] + lateness[k])
+    return time.perf_counter() - t0, np.array(lat), [h.results for h in handles]
+
+
+def serving_errors(C, trees, reqs, gpus_bf, outs, pick):
+    """Median relative error per kernel against float32 brute force with compensated
+    sums, on the first 2048 queries of each picked request.  Gravity: |e|/|ref|;
+    winding number: |e|/max(|ref|, 1); smooth distance: the error of
+    D = -log(S)/alpha, the distance the sum S stands for (a non-positive estimate
+    of S counts as an infinite error)."""
+    errs = {k: [] for k in SERVING_KERNELS}
+    for k in pick:
+        r = reqs[k]
+        n = min(r["nq"], 2048)
+        kid = {"gravity": C.GRAVITY, "wn": C.WINDING_NUMBER, "smooth": C.SMOOTH_DIST}[r["kernel"]]
+        alpha = 100.0 if r["kernel"] == "smooth" else None
+        ref, _ = gpus_bf[r["tree"]].eval(r["q"][:n], C.params(method=C.BRUTE_FORCE, kernel=kid,
+                                                               alpha=alpha))
+        est = outs[k][:n].astype(np.float64)
+        ref = ref.astype(np.float64)
+        if r["kernel"] == "wn":
+            e = np.abs(est - ref) / np.maximum(np.abs(ref), 1.0)
+        elif r["kernel"] == "gravity":
+            e = np.abs(est - ref) / np.abs(ref)
+        else:
+            ok = ref > 0
+            d_ref = -np.log(ref[ok]) / 100.0
+            with np.errstate(divide="ignore", invalid="ignore"):
+                d_est = np.where(est[ok] > 0, -np.log(np.maximum(est[ok], 1e-300)) / 100.0, np.inf)
+            e = np.abs(d_est - d_ref) / np.abs(d_ref)
+        errs[r["kernel"]].append(e)
+    return {k: (float(np.median(np.concatenate(v))) if v else None) for k, v in errs.items()}
+
+
+def run_serving(args):
+    import sbh_capi as C
+    import sbh_workloads as W
+    t_setup = time.perf_counter()
+    trees, reqs = serving_setup(C)
+    gpus = {i: C.GpuTree(t["bh"]) for i, t in enumerate(trees)}
+    server = C.Server(slots=3, slot_queries=1 << 20, max_requests_per_batch=4096)
+    ids = {}
+    for i, t in enumerate(trees):
+        ids[(i, "sbh")] = server.add_tree(t["sbh"])
+        ids[(i, "bh")] = server.add_tree(t["bh"])
+    setup_s = time.perf_counter() - t_setup
+    total_q = sum(r["nq"] for r in reqs)
+    # Warm up every path once on a slice of the stream.
+    warm = reqs[:50]
+    drive_plain(C, W, trees, warm, gpus, np.zeros(len(warm)))
+    drive_served(C, W, trees, warm, server, ids, np.zeros(len(warm)), "bh")
+    drive_served(C, W, trees, warm, server, ids, np.zeros(len(warm)), "sbh")
+    # Capacity of the plain path: every request queued at t = 0 (the first pass
+    # also grows every tree's cached workspace to its largest request).
+    drive_plain(C, W, trees, reqs, gpus, np.zeros(len(reqs)))
+    mk, _, plain_outs = drive_plain(C, W, trees, reqs, gpus, np.zeros(len(reqs)))
+    plain_rps = len(reqs) / mk
+    rng = np.random.default_rng(5)
+    pick = [k for k in rng.permutation(len(reqs))[:90]]
+    results = {"plain_bh_capacity": {"queries_per_s": total_q / mk, "requests_per_s": plain_rps,
+                                     "median_rel_err": serving_errors(C, trees, reqs, gpus,
+                                                                      plain_outs, pick)}}
+    for factor in (0.5, 1.0, 2.0, 8.0):
+        rate = factor * plain_rps
+        gaps = rng.exponential(1.0 / rate, len(reqs))
+        arrivals = np.cumsum(gaps) - gaps[0]
+        row = {"arrival_rate_rps": rate}
+        for name, fn in (("plain_bh", lambda: drive_plain(C, W, trees, reqs, gpus, arrivals)),
+                         ("served_bh", lambda: drive_served(C, W, trees, reqs, server, ids,
+                                                            arrivals, "bh")),
+                         ("served_sbh", lambda: drive_served(C, W, trees, reqs, server, ids,
+                                                             arrivals, "sbh"))):
+            mk, lat, outs = fn()
+            row[name] = {"queries_per_s": total_q / mk, "p50_ms": float(np.percentile(lat, 50)),
+                         "p99_ms": float(np.percentile(lat, 99)), "makespan_s": mk}
+            if factor == 8.0:
+                row[name]["median_rel_err"] = serving_errors(C, trees, reqs, gpus, outs, pick)
+        results[f"rate_x{factor}"] = row
+    stats = server.stats()
+    server.close()
+    hi = results["rate_x8.0"]
+    return {
+        "metric": METRIC, "value": hi["served_sbh"]["queries_per_s"], "unit": "queries/s",
+        "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": hi["served_sbh"]["makespan_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generators)",
+        "config": {"workload": "serving: 32 resident trees (16 3D, 16 2D), 1500 Poisson requests, "
+                               "gravity / winding number / smooth distance (alpha 100), 1..1e5 "
+                               "queries log-uniform, budget 64/256/1024; served SBH and BH vs "
+                               "plain per-call BH (theta 0.5)",
+                   "requests": len(reqs), "queries": total_q, "setup_s": setup_s,
+                   "server": {"slots": 3, "slot_queries": 1 << 20}},
+        "serving": results, "server_stats": stats,
+    }
+
+
+# ---------------------------------------------------------------- batching
+
+def run_batching(args):
+    import torch
+
+    import sbh_capi as C
+    import sbh_workloads as W
+    rng = np.random.default_rng(44)
+    probs = []
+    for i in range(256):
+        n = int(np.exp(rng.uniform(np.log(1024), np.log(1 << 20))))
+        pts, nrm, m = W.gaussian_mixture(n, seed=1000 + i)
+        lo, hi = W.padded_box(pts)
+        host = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=2)
+        gpu = C.GpuTree(host)
+        budget = int(rng.choice([64, 128, 256, 512]))
+        samples = W.samples_for_budget(budget, gpu.info.root_children)
+        dq = torch.from_numpy(np.ascontiguousarray(pts.T)).cuda()
+        dm = torch.from_numpy(m).cuda()
+        out = torch.empty(n, dtype=torch.float32, device="cuda")
+        p = C.params(method=C.STOCHASTIC, kernel=C.GRAVITY, samples_per_subdomain=samples, seed=i)
+        probs.append(dict(host=host, gpu=gpu, dq=dq, dm=dm, out=out, n=n, p=p))
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    entries = [(b["gpu"], b["p"], b["dq"].data_ptr(), b["n"], b["out"].data_ptr(), 0,
+                b["dm"].data_ptr()) for b in probs]
+    total_q = sum(b["n"] for b in probs)
+    self_t = [(-b["dm"] / 0.1) for b in probs]
+
+    def batched():
+        C.eval_batch(entries, stream=sh)
+
+    def sequential():
+        for b, st in zip(probs, self_t):
+            b["gpu"].eval_device(b["dq"].data_ptr(), b["n"], b["out"].data_ptr(), b["p"], stream=sh)
+            b["out"].sub_(st)
+
+    res = {}
+    for name, fn in (("one_batch_launch", batched), ("sequential_plain_calls", sequential)):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(max(1, args.steps // 4)):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = statistics.mean(ts)
+        res[name] = {"ms": ms, "queries_per_s": total_q / (ms / 1e3), "problems_per_s": 256 / (ms / 1e3)}
+    return {
+        "metric": METRIC, "value": res["one_batch_launch"]["queries_per_s"], "unit": "queries/s",
+        "n_gpus": 1, "steps": max(1, args.steps // 4), "warmup": args.warmup,
+        "ms_per_step": res["one_batch_launch"]["ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": "batching: 256 3D gravity problems, 1,024..1,048,576 sources "
+                               "log-uniform, queries = sources (self term excluded), stochastic "
+                               "BH budget 64-512, Octree2", "queries": total_q},
+        "batching": res,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sbh_wn")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "batching"],
+                    default="sbh_wn")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -509,6 +767,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.workload in ("serving", "batching") and args.impl == "ours":
+        out = run_serving(args) if args.workload == "serving" else run_batching(args)
+        print(json.dumps(out), flush=True)
+        return
+    if args.workload in ("serving", "batching"):
+        ap.error("--impl reference runs the default workloads only")
     wl = dict(WORKLOADS[args.workload])
     if args.nq:
         wl["nq"] = args.nq

@@ -10,6 +10,8 @@ produce the workloads this library is measured on, all seeded numpy
   and equal area weights (winding-number workload);
 * ``circle_points``: points on the unit circle with Gaussian jitter (2D smooth
   distance workload);
+* ``sphere_surface``: uniform points on a sphere with outward normals (serving
+  workload);
 * ``uniform_queries``: queries uniform in a box;
 * ``padded_box``: the points' bounding box grown by 0.01, as the reference's
   example does (python/example.py:23-24).
@@ -65,6 +67,15 @@ def torus_surface(n: int, seed: int, R: float = 0.6, r: float = 0.2, jitter: flo
         pts = pts + rng.normal(0.0, jitter, pts.shape)
     area = np.full(n, 4 * np.pi ** 2 * R * r / n)
     return pts.astype(np.float32), nrm.astype(np.float32), area.astype(np.float32)
+
+
+def sphere_surface(n: int, seed: int, radius: float = 0.8):
+    """Uniform samples of a sphere with outward normals and area weights 4 pi r^2 / n."""
+    rng = np.random.default_rng(seed)
+    nrm = rng.normal(size=(n, 3))
+    nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-12)
+    area = np.full(n, 4 * np.pi * radius ** 2 / n)
+    return (radius * nrm).astype(np.float32), nrm.astype(np.float32), area.astype(np.float32)
 
 
 def circle_points(n: int, seed: int, jitter: float = 1e-3):
