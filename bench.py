@@ -750,13 +750,112 @@ def run_batching(args):
     }
 
 
+# ---------------------------------------------------------- differentiation
+
+def run_differentiation(args):
+    """Smooth distance (alpha 100, max-shifted) forward and backward through the
+    autograd wrapper: stochastic BH (budget 128, Octree2/Quadtree2) and
+    deterministic BH (theta 0.5, Octree1/Quadtree1), 3D torus and 2D circle."""
+    import torch
+
+    import sbh_capi as C
+    import sbh_torch
+    import sbh_workloads as W
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    cases = []
+    pts3, nrm3, a3 = W.torus_surface(524288, seed=301, jitter=1e-3)
+    q3 = W.uniform_queries(1 << 20, seed=302, dim=3, lo=-1.0, hi=1.0)
+    pts2, nrm2, a2 = W.circle_points(262144, seed=303, jitter=1e-3)
+    q2 = W.uniform_queries(1 << 20, seed=304, dim=2, lo=-1.5, hi=1.5)
+    for dim, pts, nrm, a, q in ((3, pts3, nrm3, a3, q3), (2, pts2, nrm2, a2, q2)):
+        lo, hi = W.padded_box(pts)
+        trees = {dsl: C.GpuTree(C.HostTree(pts, nrm, a, lo, hi, alpha=100.0, dim_split_log=dsl))
+                 for dsl in (1, 2)}
+        cases.append((dim, trees, q))
+    res = {}
+    total_q = 0
+    total_ms = {"stochastic": 0.0, "barnes_hut": 0.0}
+    clocks = None
+    for dim, trees, q in cases:
+        nq = q.shape[0]
+        total_q += nq
+        tq = torch.from_numpy(q).to(dev).requires_grad_(True)
+        gout = torch.ones(nq, dtype=torch.float32, device=dev)
+        sub = q[:4096]
+        ref_v, ref_g, _ = trees[1].eval_grad(sub, C.params(method=C.BRUTE_FORCE,
+                                                            kernel=C.SMOOTH_DIST))
+        for method, tree, kw in (("stochastic", trees[2], {"budget": 128, "seed": 7}),
+                                 ("barnes_hut", trees[1], {"beta": 2.0})):
+            def step():
+                tq.grad = None
+                d = sbh_torch.smooth_distance(tree, tq, method=method, **kw)
+                d.backward(gout)
+                return d
+
+            for _ in range(args.warmup):
+                flush.zero_()
+                step()
+            tree.check(stream.cuda_stream)
+            torch.cuda.synchronize(dev)
+            ev = []
+            with ClockSampler(0) as cs:
+                for _ in range(args.steps):
+                    flush.zero_()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    step()
+                    e1.record(stream)
+                    ev.append((e0, e1))
+                torch.cuda.synchronize(dev)
+            clocks = cs.summary() if clocks is None else clocks
+            tree.check(stream.cuda_stream)
+            ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+            total_ms[method] += ms
+            # accuracy on the first 4096 queries against compensated brute force
+            p = C.params(method={"stochastic": C.STOCHASTIC, "barnes_hut": C.BARNES_HUT}[method],
+                         kernel=C.SMOOTH_DIST, beta=kw.get("beta", 2.0), seed=7,
+                         samples_per_subdomain=W.samples_for_budget(
+                             128, tree.info.root_children))
+            v, g, _ = tree.eval_grad(sub, p)
+            ok = np.isfinite(v)
+            d_err = np.abs(v[ok] - ref_v[ok]) / np.maximum(np.abs(ref_v[ok]), 1e-30)
+            g_err = (np.linalg.norm(g[ok] - ref_g[ok], axis=1) /
+                     np.maximum(np.linalg.norm(ref_g[ok], axis=1), 1e-30))
+            res[f"{dim}d_{method}"] = {
+                "fwd_bwd_ms": ms, "queries_per_s": nq / (ms / 1e3),
+                "median_rel_err_D": float(np.median(d_err)),
+                "median_rel_err_grad": float(np.median(g_err)),
+                "nonfinite_frac": float(1.0 - ok.mean()),
+                "samples_per_subdomain": int(p.samples_per_subdomain) if method == "stochastic"
+                else None}
+    value = total_q / (total_ms["stochastic"] / 1e3)
+    return {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms["stochastic"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": "differentiation: smooth distance alpha 100 (max-shifted), forward "
+                               "+ backward through torch.autograd; 3D torus 524,288 points "
+                               "(jitter 1e-3), 2D circle 262,144 points, 1,048,576 queries each; "
+                               "stochastic BH budget 128 (value) and BH theta 0.5",
+                   "l2": "flushed between steps (512 MiB write)",
+                   "accuracy_reference": "compensated FP32 brute force on the GPU, 4096 queries"},
+        "differentiation": res, "clocks": clocks,
+        "gpu_launches": 6,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "batching"],
+    ap.add_argument("--workload",
+                    choices=sorted(WORKLOADS) + ["serving", "batching", "differentiation"],
                     default="sbh_wn")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
@@ -767,11 +866,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    if args.workload in ("serving", "batching") and args.impl == "ours":
-        out = run_serving(args) if args.workload == "serving" else run_batching(args)
-        print(json.dumps(out), flush=True)
+    systems = {"serving": run_serving, "batching": run_batching,
+               "differentiation": run_differentiation}
+    if args.workload in systems and args.impl == "ours":
+        print(json.dumps(systems[args.workload](args)), flush=True)
         return
-    if args.workload in ("serving", "batching"):
+    if args.workload in systems:
         ap.error("--impl reference runs the default workloads only")
     wl = dict(WORKLOADS[args.workload])
     if args.nq:

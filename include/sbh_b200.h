@@ -264,6 +264,31 @@ int sbh_eval_device_static_scratch(sbh_gpu_tree* tree, const sbh_params* params,
  * violation recorded by earlier calls on this tree. */
 int sbh_gpu_tree_check(sbh_gpu_tree* tree, void* stream);
 
+/* ---- values and query-position gradients -------------------------------------
+ * No counterpart in the reference (its gravityGrad, include/kernel.h:61-66, is
+ * unused and is not the derivative of gravityPotential).  Any method; kernels:
+ *   GRAVITY, PLUMMER  values: the potential, as sbh_eval computes it (bit for bit
+ *                     for Barnes-Hut); grads: its analytic gradient in q,
+ *                     summed over the same terms;
+ *   SMOOTH_DIST       values: the smooth distance D = -log(S) / alpha of the sum
+ *                     S = sum_i exp(-alpha |p_i - q|) (the quantity the
+ *                     reference's callers form, python/example.py:79), with S
+ *                     held max-shifted so no term underflows; grads:
+ *                     dD/dq = sum_i w_i (q - p_i)/|q - p_i| / sum_i w_i.
+ *                     A non-positive stochastic estimate of S gives NaN.
+ * WINDING_NUMBER returns SBH_ERR_UNSUPPORTED.  The stochastic method walks the
+ * same sampled paths as sbh_eval with the same seed and differentiates every
+ * term with the path weights held fixed, which keeps the gradient of the sum
+ * unbiased.  grads: [dim][nq] float32 or NULL (values only).  Host buffers,
+ * blocking (as sbh_eval) ... */
+int sbh_eval_grad(sbh_gpu_tree* tree, const sbh_params* params, const float* queries, int64_t nq,
+                  float* values, float* grads, int32_t* contribs, float* kernel_ms,
+                  void* stream);
+/* ... or device buffers, asynchronous (as sbh_eval_device). */
+int sbh_eval_grad_device(sbh_gpu_tree* tree, const sbh_params* params, const float* d_queries,
+                         int64_t nq, float* d_values, float* d_grads, int32_t* d_contribs,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,11 @@ def oracle_lib() -> ctypes.CDLL:
         lib.orc_brute_force_f64.argtypes = [_P, _P, _P, _I64, ctypes.c_int, ctypes.c_int, _F, _F,
                                             _P, _I64, _P]
         lib.orc_brute_force_abs_f64.argtypes = lib.orc_brute_force_f64.argtypes
+        lib.orc_bh_grad.argtypes = [_P, ctypes.c_int, _P, _I64, _F, _F, _F, _P, _P, _P]
+        lib.orc_sbh_grad.argtypes = [_P, ctypes.c_int, _P, _I64, ctypes.c_int, ctypes.c_uint64,
+                                     _F, _F, _P, _P, _P]
+        lib.orc_brute_force_grad_f64.argtypes = [_P, _P, _I64, ctypes.c_int, ctypes.c_int, _F, _F,
+                                                 _P, _I64, _P, _P]
         lib.orc_philox4x32_10.argtypes = [_P, _P, _P]
         lib.orc_mt19937_stream.argtypes = [ctypes.c_uint32, _I64, _P, _P]
         lib._typed = True
@@ -217,6 +222,31 @@ class OracleTree(_TreeBase):
         return out, cnt
 
 
+    def bh_grad(self, kernel, queries, beta, alpha=1.0, eps=1e-3):
+        """Barnes-Hut value and gradient in FP64 over the reference's node set:
+        (val[nq], grad[nq, dim], counts)."""
+        q = _f32(queries, (-1, self.dim))
+        nq = q.shape[0]
+        val = np.zeros(nq, np.float64)
+        grad = np.zeros((nq, self.dim), np.float64)
+        cnt = np.zeros(nq, np.int32)
+        self.lib.orc_bh_grad(self._h, kernel, _ptr(q), nq, float(np.float32(beta)), eps,
+                             float(np.float32(alpha)), _ptr(val), _ptr(grad), _ptr(cnt))
+        return val, grad, cnt
+
+    def sbh_grad(self, kernel, queries, samples, seed=0, alpha=1.0, eps=1e-3):
+        """Stochastic estimator value and gradient on the Philox paths of sbh():
+        (val[nq], grad[nq, dim], counts)."""
+        q = _f32(queries, (-1, self.dim))
+        nq = q.shape[0]
+        val = np.zeros(nq, np.float64)
+        grad = np.zeros((nq, self.dim), np.float64)
+        cnt = np.zeros(nq, np.int32)
+        self.lib.orc_sbh_grad(self._h, kernel, _ptr(q), nq, samples, seed, eps,
+                              float(np.float32(alpha)), _ptr(val), _ptr(grad), _ptr(cnt))
+        return val, grad, cnt
+
+
 class RefTree(_TreeBase):
     """The reference's own PyQuadtree/PyOctree (include/py_tree.h) built in oracle/_ref."""
 
@@ -302,6 +332,23 @@ def brute_force_f64(points, normals, masses, kernel, queries, alpha=1.0, eps=1e-
     fn(_ptr(pts), _ptr(nrm), _ptr(m), n, dim, kernel, float(np.float32(alpha)),
        float(np.float32(eps)), _ptr(q), q.shape[0], _ptr(out))
     return out
+
+
+def brute_force_grad_f64(points, masses, kernel, queries, alpha=1.0, eps=1e-3):
+    """FP64 value and query gradient over every source: (val[nq], grad[nq, dim]).
+    Smooth distance: D = -log(sum exp(-alpha r)) / alpha and dD/dq."""
+    lib = oracle_lib()
+    pts = _f32(points)
+    dim = pts.shape[1]
+    n = pts.shape[0]
+    m = _f32(masses, (n,))
+    q = _f32(queries, (-1, dim))
+    val = np.zeros(q.shape[0], np.float64)
+    grad = np.zeros((q.shape[0], dim), np.float64)
+    lib.orc_brute_force_grad_f64(_ptr(pts), _ptr(m), n, dim, kernel, float(np.float32(alpha)),
+                                 float(np.float32(eps)), _ptr(q), q.shape[0], _ptr(val),
+                                 _ptr(grad))
+    return val, grad
 
 
 def philox4x32_10(ctr, key):

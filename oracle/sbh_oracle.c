@@ -201,6 +201,57 @@ static float kern_node(const orc_tree* t, int kernel, int64_t v, const float* q,
               t->aalpha[v], q, eps);
 }
 
+/* Value and query-position gradient of one term in FP64 (the gradient oracles):
+ *   gravity  -m / (r + 0.1)        grad  -m d / (r (r + 0.1)^2)
+ *   Plummer  m / sqrt(r^2 + eps^2)  grad  m d / (r^2 + eps^2)^(3/2)
+ *   smooth   exp(-alpha r)          grad  alpha exp(-alpha r) d / r
+ * with d = p - q and r = |d|; the gradient of a term at r = 0 is 0 (gravity,
+ * smooth).  No reference counterpart: include/kernel.h:61-66 (gravityGrad) is
+ * unused and is not the derivative of gravityPotential. */
+static double kern_grad64(int kernel, int dim, const float* p, float m, float a, const float* q,
+                          float eps, double* g) {
+  double d[3] = {0, 0, 0}, ss = 0;
+  for (int k = 0; k < dim; k++) {
+    d[k] = (double)p[k] - (double)q[k];
+    ss += d[k] * d[k];
+  }
+  const double r = sqrt(ss);
+  double v, c;
+  switch (kernel) {
+    case ORC_GRAVITY: {
+      const double rs = r + (double)1e-1f;
+      v = -(double)m / rs;
+      c = r > 0 ? -(double)m / (r * rs * rs) : 0;
+      break;
+    }
+    case ORC_SMOOTH_DIST:
+      v = exp(-(double)a * r);
+      c = r > 0 ? (double)a * v / r : 0;
+      break;
+    default: {
+      const double s2 = ss + (double)eps * (double)eps;
+      v = (double)m / sqrt(s2);
+      c = (double)m / (s2 * sqrt(s2));
+      break;
+    }
+  }
+  for (int k = 0; k < dim; k++) g[k] = c * d[k];
+  return v;
+}
+
+/* Final form of a (sum, gradient-of-sum) pair: the potential as is, or for the
+ * smooth distance D = -log(S) / alpha and dD/dq = -(dS/dq) / (alpha S). */
+static void finish_grad(int kernel, int dim, float alpha, double S, const double* gS,
+                        double* val, double* grad) {
+  if (kernel == ORC_SMOOTH_DIST) {
+    *val = -log(S) / (double)alpha;
+    for (int k = 0; k < dim; k++) grad[k] = -gS[k] / ((double)alpha * S);
+  } else {
+    *val = S;
+    for (int k = 0; k < dim; k++) grad[k] = gS[k];
+  }
+}
+
 /* ---------------------------------------------------------------- build */
 
 static void grow(orc_tree* t, int64_t need) {
@@ -617,6 +668,85 @@ void orc_bh(const orc_tree* t, int kernel, const float* q, int64_t nq, float bet
   par_for(nq, 16, bh_body, &c);
 }
 
+/* Barnes-Hut value and gradient: the node set of evaluateBarnesHut_stackless
+ * (include/barnes_hut.h:23-78, bh_one above), every accepted term taken in
+ * FP64 with its gradient (kern_grad64). */
+static void bh_grad_one(const orc_tree* t, int kernel, const float* q, float beta, float eps,
+                        float alpha, double* val, double* grad, int32_t* ncontrib) {
+  enum { FROM_CHILD, FROM_PARENT, FROM_SIBLING };
+  const int dim = t->dim;
+  double S = 0, gS[3] = {0, 0, 0}, g[3];
+  int nc = 0;
+  int64_t node = 0;
+  int state = FROM_PARENT;
+  int64_t guard = 8 * t->nn + 64;
+  while (guard-- > 0) {
+    if (state != FROM_CHILD) {
+      if (far_field_ratio(t, node, q) >= beta) {
+        if (t->leaf[node]) {
+          for (int64_t i = t->start[node]; i < t->end[node]; i++) {
+            S += kern_grad64(kernel, dim, t->pos + i * dim, t->mass[i], alpha, q, eps, g);
+            for (int k = 0; k < dim; k++) gS[k] += g[k];
+            nc++;
+          }
+        } else {
+          S += kern_grad64(kernel, dim, t->apos + node * dim, t->amass[node], alpha, q, eps, g);
+          for (int k = 0; k < dim; k++) gS[k] += g[k];
+          nc++;
+        }
+      } else {
+        int64_t c = first_child(t, node);
+        if (c >= 0) {
+          node = c;
+          state = FROM_PARENT;
+          continue;
+        }
+      }
+    }
+    if (node == 0) {
+      finish_grad(kernel, dim, alpha, S, gS, val, grad);
+      *ncontrib = nc;
+      return;
+    }
+    int64_t p = t->parent[node];
+    int64_t nx = next_child(t, p, node);
+    if (nx < 0) {
+      node = p;
+      state = FROM_CHILD;
+    } else {
+      node = nx;
+      state = FROM_SIBLING;
+    }
+  }
+  *val = NAN;
+  *ncontrib = -1;
+}
+
+typedef struct {
+  const orc_tree* t;
+  int kernel, samples;
+  const float* q;
+  float beta, eps, alpha;
+  uint64_t seed;
+  double *val, *grad;
+  int32_t* counts;
+} grad_ctx;
+
+static void bh_grad_body(void* vc, int64_t i) {
+  grad_ctx* c = (grad_ctx*)vc;
+  const int dim = c->t->dim;
+  int32_t n = 0;
+  bh_grad_one(c->t, c->kernel, c->q + i * dim, c->beta, c->eps, c->alpha, c->val + i,
+              c->grad + i * dim, &n);
+  if (c->counts) c->counts[i] = n;
+}
+
+void orc_bh_grad(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta,
+                 float eps, float alpha, double* val, double* grad, int32_t* counts) {
+  grad_ctx c = {t, kernel, 0, q, beta, eps, alpha, 0, val, grad, counts};
+  par_for(nq, 16, bh_grad_body, &c);
+}
+
 /* evaluateBarnesHutGPUVote, include/barnes_hut_gpu.h:19-72: one traversal per
  * group; __all_sync over the group's queries decides acceptance. */
 static void bh_vote_body(void* vc, int64_t g) {
@@ -898,6 +1028,118 @@ void orc_sbh(const orc_tree* t, int kernel, const float* q, int64_t nq, int samp
   par_for(nq, 16, sbh_body, &c);
 }
 
+/* The stochastic estimator's value and gradient on the Philox paths of
+ * sbh_one (same float path decisions and weights, include/tree_sampler.h:21-113);
+ * every kernel term is taken in FP64 with its gradient and weighted by the
+ * float path weight. */
+static void sbh_grad_one(const orc_tree* t, int kernel, const float* q, int samples,
+                         orc_rng* rng, float eps, float alpha, double* val, double* grad,
+                         int32_t* total_contribs) {
+  const int dim = t->dim;
+  double bh = 0, gbh[3] = {0, 0, 0}, ml = 0, gml[3] = {0, 0, 0}, g[3];
+  int tc = 0;
+  if (t->leaf[0]) {
+    finish_grad(kernel, dim, alpha, 0, gbh, val, grad);
+    *total_contribs = 0;
+    return;
+  }
+  const uint64_t* rm = t->mask;
+  uint32_t sub_ordinal = 0;
+  for (uint64_t b = first_bit(rm, t->mw, t->bf); b < (uint64_t)t->bf;
+       b = next_bit(rm, t->mw, t->bf, b), sub_ordinal++) {
+    int64_t S = t->child[b];
+    if (t->leaf[S]) {
+      for (int64_t i = t->start[S]; i < t->end[S]; i++) {
+        bh += kern_grad64(kernel, dim, t->pos + i * dim, t->mass[i], alpha, q, eps, g);
+        for (int k = 0; k < dim; k++) gbh[k] += g[k];
+        tc++;
+      }
+    } else {
+      bh += kern_grad64(kernel, dim, t->apos + S * dim, t->amass[S], alpha, q, eps, g);
+      for (int k = 0; k < dim; k++) gbh[k] += g[k];
+      tc++;
+    }
+    uint64_t nS = (uint64_t)(t->end[S] - t->start[S]);
+    double sub = 0, gsub[3] = {0, 0, 0};
+    for (int ss = 0; ss < samples; ss++) {
+      rng_begin_path(rng, sub_ordinal * (uint32_t)samples + (uint32_t)ss);
+      int64_t idx = (int64_t)rng_index(rng, nS) + t->start[S];
+      float spi = (float)nS;
+      const float* sp = t->pos + idx * dim;
+      float ev = 1;
+      int64_t prev = S, cur = S;
+      float r0 = far_field_ratio(t, cur, q);
+      float cb = (1.0f < r0) ? r0 : 1.0f;
+      while (!t->leaf[cur]) {
+        float ffr = far_field_ratio(t, cur, q);
+        float ratio = cb / ffr;
+        float tp = (1.0f < ratio) ? 1.0f : ratio;
+        float p = rng_uniform(rng);
+        if (p > tp) break;
+        ev *= tp;
+        prev = cur;
+        cur = contained_in_child(t, prev, sp);
+        if (cur < 0) {
+          *val = NAN;
+          *total_contribs = -1;
+          return;
+        }
+        cb = (cb < ffr) ? ffr : cb;
+        double gp[3];
+        double diff = -kern_grad64(kernel, dim, t->apos + prev * dim, t->amass[prev], alpha, q,
+                                   eps, gp);
+        double gdiff[3] = {-gp[0], -gp[1], -gp[2]};
+        const uint64_t* pm = t->mask + prev * t->mw;
+        for (uint64_t cbit = first_bit(pm, t->mw, t->bf); cbit < (uint64_t)t->bf;
+             cbit = next_bit(pm, t->mw, t->bf, cbit)) {
+          int64_t c = t->child[prev * t->bf + cbit];
+          if (t->leaf[c]) {
+            for (int64_t i = t->start[c]; i < t->end[c]; i++) {
+              diff += kern_grad64(kernel, dim, t->pos + i * dim, t->mass[i], alpha, q, eps, g);
+              for (int k = 0; k < dim; k++) gdiff[k] += g[k];
+              tc++;
+            }
+          } else {
+            diff += kern_grad64(kernel, dim, t->apos + c * dim, t->amass[c], alpha, q, eps, g);
+            for (int k = 0; k < dim; k++) gdiff[k] += g[k];
+            tc++;
+          }
+        }
+        const double w = (double)(spi / (ev * (float)(uint64_t)(t->end[prev] - t->start[prev])));
+        sub += w * diff;
+        for (int k = 0; k < dim; k++) gsub[k] += w * gdiff[k];
+      }
+    }
+    ml += sub / samples;
+    for (int k = 0; k < dim; k++) gml[k] += gsub[k] / samples;
+  }
+  for (int k = 0; k < dim; k++) gbh[k] += gml[k];
+  finish_grad(kernel, dim, alpha, bh + ml, gbh, val, grad);
+  *total_contribs = tc;
+}
+
+static void sbh_grad_body(void* vc, int64_t i) {
+  grad_ctx* c = (grad_ctx*)vc;
+  const int dim = c->t->dim;
+  orc_rng r;
+  memset(&r, 0, sizeof(r));
+  r.mode = ORC_RNG_PHILOX;
+  r.key[0] = (uint32_t)c->seed;
+  r.key[1] = (uint32_t)(c->seed >> 32);
+  r.query = (uint64_t)i;
+  int32_t n = 0;
+  sbh_grad_one(c->t, c->kernel, c->q + i * dim, c->samples, &r, c->eps, c->alpha, c->val + i,
+               c->grad + i * dim, &n);
+  if (c->counts) c->counts[i] = n;
+}
+
+void orc_sbh_grad(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
+                  uint64_t seed, float eps, float alpha, double* val, double* grad,
+                  int32_t* counts) {
+  grad_ctx c = {t, kernel, samples, q, 0, eps, alpha, seed, val, grad, counts};
+  par_for(nq, 16, sbh_grad_body, &c);
+}
+
 /* ------------------------------------------------------------ brute force */
 
 typedef struct {
@@ -935,4 +1177,31 @@ void orc_brute_force_abs_f64(const float* pts, const float* nrm, const float* ma
                              int64_t nq, double* out) {
   bf_ctx c = {pts, nrm, mass, q, n, dim, kernel, 1, alpha, eps, out};
   par_for(nq, 8, bf_body, &c);
+}
+
+typedef struct {
+  const float *pts, *mass, *q;
+  int64_t n;
+  int dim, kernel;
+  float alpha, eps;
+  double *val, *grad;
+} bf_grad_ctx;
+
+static void bf_grad_body(void* vc, int64_t j) {
+  bf_grad_ctx* c = (bf_grad_ctx*)vc;
+  const int dim = c->dim;
+  double S = 0, gS[3] = {0, 0, 0}, g[3];
+  for (int64_t i = 0; i < c->n; i++) {
+    S += kern_grad64(c->kernel, dim, c->pts + i * dim, c->mass[i], c->alpha, c->q + j * dim,
+                     c->eps, g);
+    for (int k = 0; k < dim; k++) gS[k] += g[k];
+  }
+  finish_grad(c->kernel, dim, c->alpha, S, gS, c->val + j, c->grad + j * dim);
+}
+
+void orc_brute_force_grad_f64(const float* pts, const float* mass, int64_t n, int dim,
+                              int kernel, float alpha, float eps, const float* q, int64_t nq,
+                              double* val, double* grad) {
+  bf_grad_ctx c = {pts, mass, q, n, dim, kernel, alpha, eps, val, grad};
+  par_for(nq, 8, bf_grad_body, &c);
 }

@@ -76,6 +76,22 @@ void orc_brute_force_abs_f64(const float* pts, const float* nrm, const float* ma
                              int dim, int kernel, float alpha, float eps, const float* q,
                              int64_t nq, double* out);
 
+/* Values and query-position gradients (FP64 accumulation), kernels gravity,
+ * Plummer and smooth distance.  val[nq]; grad row-major [nq][dim].  For the
+ * smooth kernel val is D = -log(S)/alpha and grad dD/dq; otherwise the
+ * potential and its gradient.  orc_bh_grad takes Barnes-Hut's node set;
+ * orc_sbh_grad the stochastic estimator on orc_sbh's Philox paths (same seed,
+ * same paths), differentiating every term with the path weights held fixed;
+ * orc_brute_force_grad_f64 every source. */
+void orc_bh_grad(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta,
+                 float eps, float alpha, double* val, double* grad, int32_t* counts);
+void orc_sbh_grad(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
+                  uint64_t seed, float eps, float alpha, double* val, double* grad,
+                  int32_t* counts);
+void orc_brute_force_grad_f64(const float* pts, const float* mass, int64_t n, int dim,
+                              int kernel, float alpha, float eps, const float* q, int64_t nq,
+                              double* val, double* grad);
+
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void orc_mt19937_stream(uint32_t seed, int64_t n, uint32_t* raw, float* uniform01);
 int orc_num_threads(void);

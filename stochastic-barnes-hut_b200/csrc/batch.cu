@@ -139,7 +139,7 @@ template <int DIM, int K>
 __device__ __noinline__ void run_sbh(const DevTree& t, const BatchItem& it, long long u,
                                      const int* ord, float* scratch, int* status) {
   const int lane = threadIdx.x & 31;
-  const SbhWarpSmem ws = sbh_carve(scratch, t.root_children);
+  const SbhWarpSmem<float> ws = sbh_carve<float>(scratch, t.root_children);
   const long long s0 = u * kUnitQueriesSampler;
   const long long s1 = min(it.nq, s0 + kUnitQueriesSampler);
   for (long long s = s0; s < s1; s++) {
@@ -259,7 +259,7 @@ BatchEngine::BatchEngine(const Limits& lim, int sm_count) : lim_(lim), sm_count_
   // Per-warp shared memory: the tree record, then the larger of the
   // Barnes-Hut stack and the sampler's scratch.
   const int stack_words = (lim_.max_tree_depth + 2) * (int)sizeof(BhStackEntry) / 4;
-  const int scratch = std::max(stack_words, sbh_warp_words(lim_.max_root_children));
+  const int scratch = std::max(stack_words, sbh_warp_words<float>(lim_.max_root_children));
   const int warp_words = kTreeWords + (scratch + 3) / 4 * 4;
   eval_smem_ = (size_t)kEvalWarps * warp_words * sizeof(float);
   if (eval_smem_ > 48 * 1024)
@@ -324,7 +324,7 @@ cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status) {
   const int aux_blocks = sm_count_ * 4;
   const int stack_cap = lim_.max_tree_depth + 2;
   const int stack_words = stack_cap * (int)sizeof(BhStackEntry) / 4;
-  const int scratch = std::max(stack_words, sbh_warp_words(lim_.max_root_children));
+  const int scratch = std::max(stack_words, sbh_warp_words<float>(lim_.max_root_children));
   const int warp_words = kTreeWords + (scratch + 3) / 4 * 4;
   cudaMemsetAsync(d_hist_, 0, sizeof(unsigned) * max_buckets(lim_), stream);
   batch_keys_kernel<<<aux_blocks, kAuxThreads, 0, stream>>>(d_header_, d_items_, d_keys_, d_hist_);

@@ -31,9 +31,11 @@ bool wants_sort(const sbh_params* p) {
   return p->method == SBH_METHOD_BARNES_HUT || p->method == SBH_METHOD_STOCHASTIC;
 }
 
+// Enqueues one evaluation.  With `grad` the adjoint kernels run instead (values
+// and, when d_grads is non-null, gradients).
 cudaError_t run_eval(sbh_gpu_tree* tree, const sbh_params* p, const float* d_q, int64_t nq,
                      float* d_out, int* d_contribs, int* d_order, void* d_sortws,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, bool grad = false, float* d_grads = nullptr) {
   const sbh::DevTree& t = tree->dev;
   sbh::KParams kp;
   kp.alpha = std::isnan(p->alpha) ? t.alpha : p->alpha;
@@ -44,6 +46,10 @@ cudaError_t run_eval(sbh_gpu_tree* tree, const sbh_params* p, const float* d_q, 
     if (e != cudaSuccess) return e;
     order = d_order;
   }
+  if (grad)
+    return sbh::launch_gradient(t, p->method, p->kernel, d_q, nq, order, p->beta,
+                                p->samples_per_subdomain, p->seed, kp, d_out, d_grads, d_contribs,
+                                tree->d_status, stream, tree->sm_count);
   switch (p->method) {
     case SBH_METHOD_BRUTE_FORCE: {
       cudaError_t e =
@@ -62,6 +68,111 @@ cudaError_t run_eval(sbh_gpu_tree* tree, const sbh_params* p, const float* d_q, 
                                     tree->sm_count);
   }
   return cudaErrorInvalidValue;
+}
+
+// Extra checks of the gradient entry points.
+int check_grad_params(const sbh_gpu_tree* tree, const sbh_params* p) {
+  if (p->kernel == SBH_KERNEL_WINDING_NUMBER)
+    return sbh::fail(SBH_ERR_UNSUPPORTED, "gradients of gravity, Plummer and smooth distance only");
+  if (p->method == SBH_METHOD_STOCHASTIC &&
+      sbh::gradient_smem_bytes(tree->dev, p->kernel) > 227 * 1024)
+    return sbh::fail(SBH_ERR_UNSUPPORTED, "root too wide for the stochastic gradient kernel");
+  return SBH_OK;
+}
+
+// sbh_eval and sbh_eval_grad: host buffers, blocking.
+int blocking_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* queries, int64_t nq,
+                  float* results, float* grads, int32_t* contribs, float* kernel_ms,
+                  void* stream_ptr, bool grad) {
+  int st = sbh::check_eval_params(tree, params, nq);
+  if (st == SBH_OK && grad) st = check_grad_params(tree, params);
+  if (st != SBH_OK) return st;
+  if (nq > 0 && (!queries || !results))
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
+  if (kernel_ms) *kernel_ms = 0.f;
+  if (nq == 0) return sbh::ok();
+  std::lock_guard<std::mutex> lock(tree->mu);
+  DeviceGuard guard(tree->device);
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  const int dim = tree->dev.dim;
+  const size_t b_q = align256((size_t)dim * nq * sizeof(float));
+  const size_t b_out = align256((size_t)nq * sizeof(float));
+  const size_t b_grad = grads ? b_q : 0;
+  const size_t b_cnt = contribs ? align256((size_t)nq * sizeof(int)) : 0;
+  const size_t b_ord = align256((size_t)nq * sizeof(int));
+  const size_t b_sort = align256(sbh::query_sort_workspace_bytes(nq));
+  const size_t need = b_q + b_out + b_grad + b_cnt + b_ord + b_sort;
+  if (tree->ws_bytes < need) {
+    if (tree->ws) cudaFree(tree->ws);
+    tree->ws = nullptr;
+    tree->ws_bytes = 0;
+    SBH_CK(cudaMalloc(&tree->ws, need), "cudaMalloc(workspace)");
+    tree->ws_bytes = need;
+  }
+  char* w = static_cast<char*>(tree->ws);
+  float* d_q = reinterpret_cast<float*>(w);
+  float* d_out = reinterpret_cast<float*>(w + b_q);
+  float* d_grad = grads ? reinterpret_cast<float*>(w + b_q + b_out) : nullptr;
+  int* d_cnt = contribs ? reinterpret_cast<int*>(w + b_q + b_out + b_grad) : nullptr;
+  int* d_ord = reinterpret_cast<int*>(w + b_q + b_out + b_grad + b_cnt);
+  void* d_sort = w + b_q + b_out + b_grad + b_cnt + b_ord;
+
+  SBH_CK(cudaMemcpyAsync(d_q, queries, (size_t)dim * nq * sizeof(float), cudaMemcpyHostToDevice, stream),
+         "copy queries to device");
+  SBH_CK(cudaEventRecord(tree->ev0, stream), "cudaEventRecord");
+  SBH_CK(run_eval(tree, params, d_q, nq, d_out, d_cnt, d_ord, d_sort, stream, grad, d_grad),
+         "kernel launch");
+  SBH_CK(cudaEventRecord(tree->ev1, stream), "cudaEventRecord");
+  SBH_CK(cudaMemcpyAsync(results, d_out, (size_t)nq * sizeof(float), cudaMemcpyDeviceToHost, stream),
+         "copy results to host");
+  if (grads)
+    SBH_CK(cudaMemcpyAsync(grads, d_grad, (size_t)dim * nq * sizeof(float), cudaMemcpyDeviceToHost,
+                           stream),
+           "copy gradients to host");
+  if (contribs)
+    SBH_CK(cudaMemcpyAsync(contribs, d_cnt, (size_t)nq * sizeof(int), cudaMemcpyDeviceToHost, stream),
+           "copy counts to host");
+  int status = 0;
+  SBH_CK(cudaMemcpyAsync(&status, tree->d_status, sizeof(int), cudaMemcpyDeviceToHost, stream),
+         "read status");
+  SBH_CK(cudaStreamSynchronize(stream), "evaluation");
+  if (kernel_ms) SBH_CK(cudaEventElapsedTime(kernel_ms, tree->ev0, tree->ev1), "cudaEventElapsedTime");
+  if (status != 0) {
+    cudaMemsetAsync(tree->d_status, 0, sizeof(int), stream);
+    cudaStreamSynchronize(stream);
+    return sbh::fail(SBH_ERR_DEVICE_LIMIT, "device traversal hit a bound (status bits " +
+                                               std::to_string(status) + ")");
+  }
+  return sbh::ok();
+}
+
+// sbh_eval_device and sbh_eval_grad_device: device buffers, asynchronous.
+int device_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* d_queries, int64_t nq,
+                float* d_results, float* d_grads, int32_t* d_contribs, void* stream_ptr,
+                bool grad) {
+  int st = sbh::check_eval_params(tree, params, nq);
+  if (st == SBH_OK && grad) st = check_grad_params(tree, params);
+  if (st != SBH_OK) return st;
+  if (nq == 0) return sbh::ok();
+  if (!d_queries || !d_results)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
+  DeviceGuard guard(tree->device);
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  void* tmp = nullptr;
+  int* d_ord = nullptr;
+  void* d_sort = nullptr;
+  if (wants_sort(params)) {
+    const size_t b_ord = align256((size_t)nq * sizeof(int));
+    SBH_CK(cudaMallocAsync(&tmp, b_ord + sbh::query_sort_workspace_bytes(nq), stream),
+           "cudaMallocAsync(workspace)");
+    d_ord = static_cast<int*>(tmp);
+    d_sort = static_cast<char*>(tmp) + b_ord;
+  }
+  cudaError_t e = run_eval(tree, params, d_queries, nq, d_results, d_contribs, d_ord, d_sort,
+                           stream, grad, d_grads);
+  if (tmp) cudaFreeAsync(tmp, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  return sbh::ok();
 }
 
 }  // namespace
@@ -213,83 +324,27 @@ SBH_API int sbh_gpu_tree_info(const sbh_gpu_tree* tree, sbh_tree_info* info) {
 SBH_API int sbh_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* queries,
                      int64_t nq, float* results, int32_t* contribs, float* kernel_ms,
                      void* stream_ptr) {
-  int st = sbh::check_eval_params(tree, params, nq);
-  if (st != SBH_OK) return st;
-  if (nq > 0 && (!queries || !results))
-    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
-  if (kernel_ms) *kernel_ms = 0.f;
-  if (nq == 0) return sbh::ok();
-  std::lock_guard<std::mutex> lock(tree->mu);
-  DeviceGuard guard(tree->device);
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-  const int dim = tree->dev.dim;
-  const size_t b_q = align256((size_t)dim * nq * sizeof(float));
-  const size_t b_out = align256((size_t)nq * sizeof(float));
-  const size_t b_cnt = contribs ? align256((size_t)nq * sizeof(int)) : 0;
-  const size_t b_ord = align256((size_t)nq * sizeof(int));
-  const size_t b_sort = align256(sbh::query_sort_workspace_bytes(nq));
-  const size_t need = b_q + b_out + b_cnt + b_ord + b_sort;
-  if (tree->ws_bytes < need) {
-    if (tree->ws) cudaFree(tree->ws);
-    tree->ws = nullptr;
-    tree->ws_bytes = 0;
-    SBH_CK(cudaMalloc(&tree->ws, need), "cudaMalloc(workspace)");
-    tree->ws_bytes = need;
-  }
-  char* w = static_cast<char*>(tree->ws);
-  float* d_q = reinterpret_cast<float*>(w);
-  float* d_out = reinterpret_cast<float*>(w + b_q);
-  int* d_cnt = contribs ? reinterpret_cast<int*>(w + b_q + b_out) : nullptr;
-  int* d_ord = reinterpret_cast<int*>(w + b_q + b_out + b_cnt);
-  void* d_sort = w + b_q + b_out + b_cnt + b_ord;
-
-  SBH_CK(cudaMemcpyAsync(d_q, queries, (size_t)dim * nq * sizeof(float), cudaMemcpyHostToDevice, stream),
-         "copy queries to device");
-  SBH_CK(cudaEventRecord(tree->ev0, stream), "cudaEventRecord");
-  SBH_CK(run_eval(tree, params, d_q, nq, d_out, d_cnt, d_ord, d_sort, stream), "kernel launch");
-  SBH_CK(cudaEventRecord(tree->ev1, stream), "cudaEventRecord");
-  SBH_CK(cudaMemcpyAsync(results, d_out, (size_t)nq * sizeof(float), cudaMemcpyDeviceToHost, stream),
-         "copy results to host");
-  if (contribs)
-    SBH_CK(cudaMemcpyAsync(contribs, d_cnt, (size_t)nq * sizeof(int), cudaMemcpyDeviceToHost, stream),
-           "copy counts to host");
-  int status = 0;
-  SBH_CK(cudaMemcpyAsync(&status, tree->d_status, sizeof(int), cudaMemcpyDeviceToHost, stream),
-         "read status");
-  SBH_CK(cudaStreamSynchronize(stream), "evaluation");
-  if (kernel_ms) SBH_CK(cudaEventElapsedTime(kernel_ms, tree->ev0, tree->ev1), "cudaEventElapsedTime");
-  if (status != 0) {
-    cudaMemsetAsync(tree->d_status, 0, sizeof(int), stream);
-    cudaStreamSynchronize(stream);
-    return sbh::fail(SBH_ERR_DEVICE_LIMIT, "device traversal hit a bound (status bits " +
-                                               std::to_string(status) + ")");
-  }
-  return sbh::ok();
+  return blocking_eval(tree, params, queries, nq, results, nullptr, contribs, kernel_ms,
+                       stream_ptr, false);
 }
 
 SBH_API int sbh_eval_device(sbh_gpu_tree* tree, const sbh_params* params, const float* d_queries,
                             int64_t nq, float* d_results, int32_t* d_contribs, void* stream_ptr) {
-  int st = sbh::check_eval_params(tree, params, nq);
-  if (st != SBH_OK) return st;
-  if (nq == 0) return sbh::ok();
-  if (!d_queries || !d_results)
-    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
-  DeviceGuard guard(tree->device);
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-  void* tmp = nullptr;
-  int* d_ord = nullptr;
-  void* d_sort = nullptr;
-  if (wants_sort(params)) {
-    const size_t b_ord = align256((size_t)nq * sizeof(int));
-    SBH_CK(cudaMallocAsync(&tmp, b_ord + sbh::query_sort_workspace_bytes(nq), stream),
-           "cudaMallocAsync(workspace)");
-    d_ord = static_cast<int*>(tmp);
-    d_sort = static_cast<char*>(tmp) + b_ord;
-  }
-  cudaError_t e = run_eval(tree, params, d_queries, nq, d_results, d_contribs, d_ord, d_sort, stream);
-  if (tmp) cudaFreeAsync(tmp, stream);
-  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-  return sbh::ok();
+  return device_eval(tree, params, d_queries, nq, d_results, nullptr, d_contribs, stream_ptr,
+                     false);
+}
+
+SBH_API int sbh_eval_grad(sbh_gpu_tree* tree, const sbh_params* params, const float* queries,
+                          int64_t nq, float* values, float* grads, int32_t* contribs,
+                          float* kernel_ms, void* stream_ptr) {
+  return blocking_eval(tree, params, queries, nq, values, grads, contribs, kernel_ms, stream_ptr,
+                       true);
+}
+
+SBH_API int sbh_eval_grad_device(sbh_gpu_tree* tree, const sbh_params* params,
+                                 const float* d_queries, int64_t nq, float* d_values,
+                                 float* d_grads, int32_t* d_contribs, void* stream_ptr) {
+  return device_eval(tree, params, d_queries, nq, d_values, d_grads, d_contribs, stream_ptr, true);
 }
 
 SBH_API int sbh_gpu_tree_check(sbh_gpu_tree* tree, void* stream_ptr) {

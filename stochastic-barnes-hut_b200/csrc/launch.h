@@ -19,6 +19,15 @@ cudaError_t launch_stochastic(const DevTree& t, int kernel, const float* q, long
                               const KParams& kp, float* out, int* contribs, int* status,
                               cudaStream_t stream, int sm_count);
 
+// Values and query-position gradients (adjoint.cu): method is SBH_METHOD_*,
+// kernel gravity, Plummer or smooth distance; grads is SoA [dim][nq] or null.
+cudaError_t launch_gradient(const DevTree& t, int method, int kernel, const float* q, long long nq,
+                            const int* order, float beta, int samples, unsigned long long seed,
+                            const KParams& kp, float* out, float* grads, int* contribs,
+                            int* status, cudaStream_t stream, int sm_count);
+// Dynamic shared memory per block of the stochastic gradient kernel.
+size_t gradient_smem_bytes(const DevTree& t, int kernel);
+
 // Spatial ordering of queries: order[i] is the i-th query in Morton-bucket
 // order.  `ws` must hold query_sort_workspace_bytes(nq) bytes.
 size_t query_sort_workspace_bytes(long long nq);

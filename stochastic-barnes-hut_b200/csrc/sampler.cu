@@ -53,8 +53,8 @@ __global__ void __launch_bounds__(SBH_THREADS, 8)
   extern __shared__ float s_mem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const SbhWarpSmem ws = sbh_carve(s_mem + (size_t)warp * sbh_warp_words(t.root_children),
-                                   t.root_children);
+  const SbhWarpSmem<float> ws = sbh_carve<float>(
+      s_mem + (size_t)warp * sbh_warp_words<float>(t.root_children), t.root_children);
   const long long stride = (long long)gridDim.x * SBH_WARPS;
   for (long long slot = (long long)blockIdx.x * SBH_WARPS + warp; slot < nq; slot += stride) {
     const long long qi = order ? (long long)__ldg(order + slot) : slot;
@@ -72,7 +72,7 @@ template <int DIM, int K>
 cudaError_t launch_sbh(const DevTree& t, const float* q, long long nq, const int* order,
                        int samples, unsigned long long seed, const KParams& kp, float* out,
                        int* contribs, int* status, cudaStream_t stream, int sm_count) {
-  const size_t smem = (size_t)SBH_WARPS * sbh_warp_words(t.root_children) * sizeof(float);
+  const size_t smem = (size_t)SBH_WARPS * sbh_warp_words<float>(t.root_children) * sizeof(float);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(stochastic_kernel<DIM, K>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "device_common.cuh"
+#include "sums.cuh"
 
 namespace sbh {
 
@@ -17,10 +18,9 @@ struct BhStackEntry {
 
 // Kernel value of a query's own source (mass m at the query point): the term a
 // caller excludes when the queries are the sources themselves.
-template <int DIM, int K>
-__device__ __forceinline__ float self_term(float3 q, float m, const KParams& kp) {
-  return kernel_exact<DIM, K>(make_float4(q.x, q.y, q.z, m), make_float4(0.f, 0.f, 0.f, 0.f), q,
-                              kp);
+template <int DIM, int K, class A = SumF<DIM, K>>
+__device__ __forceinline__ typename A::V self_term(float3 q, float m, const KParams& kp) {
+  return A::point(make_float4(q.x, q.y, q.z, m), make_float4(0.f, 0.f, 0.f, 0.f), q, kp);
 }
 
 // One warp evaluates the queries at sorted positions [slot0, slot_end) (at
@@ -37,15 +37,17 @@ __device__ __forceinline__ float self_term(float3 q, float m, const KParams& kp)
 // With VOTE the lanes accept a node only if all of them do, which is the
 // reference GPU kernel's __all_sync semantics (include/barnes_hut_gpu.h:34).
 // self_mass (optional, indexed like the queries) subtracts each query's own
-// source term.
-template <int DIM, int K, bool VOTE>
+// source term.  The sums follow the policy A (sums.cuh); `grads` receives the
+// gradient when A carries one.
+template <int DIM, int K, bool VOTE, class A = SumF<DIM, K>>
 __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __restrict__ qsoa,
                                              long long nq, const int* __restrict__ order,
                                              long long slot0, long long slot_end, float beta,
                                              const KParams& kp, float* __restrict__ out,
                                              int* __restrict__ contribs, int* status,
                                              BhStackEntry* stk, int stack_cap,
-                                             const float* __restrict__ self_mass) {
+                                             const float* __restrict__ self_mass,
+                                             float* __restrict__ grads = nullptr) {
   const int lane = threadIdx.x & 31;
   const long long slot = slot0 + lane;
   const bool valid = slot < slot_end;
@@ -54,7 +56,7 @@ __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __re
   const long long qi = valid ? (order ? (long long)__ldg(order + slot) : slot) : 0;
   const float3 q = valid ? load_query<DIM>(qsoa, nq, qi) : make_float3(0.f, 0.f, 0.f);
 
-  float total = 0.f;
+  typename A::V total = A::zero();
   int nc = 0;
   if (lane == 0) stk[0] = BhStackEntry{0, 1, active};
   __syncwarp();
@@ -92,11 +94,11 @@ __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __re
     if (acc) {
       if (leaf && topo.w - topo.z != 1) {
         for (int i = topo.z; i < topo.w; i++) {
-          total = radd(total, kernel_exact<DIM, K>(__ldg(t.pt_pm + i), __ldg(t.pt_nrm + i), q, kp));
+          total = A::add(total, A::point(__ldg(t.pt_pm + i), __ldg(t.pt_nrm + i), q, kp));
           nc++;
         }
       } else {
-        total = radd(total, kernel_node<DIM, K>(cm, __ldg(t.nd_agg + node), q, kp));
+        total = A::add(total, A::node(cm, __ldg(t.nd_agg + node), q, kp));
         nc++;
       }
     }
@@ -112,8 +114,8 @@ __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __re
     __syncwarp();
   }
   if (valid) {
-    if (self_mass) total = rsub(total, self_term<DIM, K>(q, __ldg(self_mass + qi), kp));
-    out[qi] = total;
+    if (self_mass) total = A::sub(total, self_term<DIM, K, A>(q, __ldg(self_mass + qi), kp));
+    A::store(out, grads, nq, qi, total, kp);
     if (contribs) contribs[qi] = nc;
   }
 }
@@ -122,20 +124,21 @@ __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __re
 
 constexpr int SBH_VCAP = 512;  // node/child values buffered per warp per pass
 
-// Per-warp shared-memory scratch of the expansion step.
+// Per-warp shared-memory scratch of the expansion step (V: the policy's value).
+template <class V>
 struct ExpandSmem {
-  float* vals;      // [SBH_VCAP] node and child values of the current pass
+  V* vals;          // [SBH_VCAP] node and child values of the current pass
   int* ent;         // [SBH_VCAP] node evaluated at each entry of the current pass
   unsigned* multi;  // [SBH_VCAP/32] entries that are leaves with several points
 };
 
 // acc += k(point) for every point of leaf tc, in order (rare: leaves with
 // several points exist only for leaf sizes > 1 or at the depth cap).
-template <int DIM, int K>
-__device__ __forceinline__ float add_leaf_points(const DevTree& t, int4 tc, float3 q,
-                                                 const KParams& kp, float acc) {
+template <class A>
+__device__ __forceinline__ typename A::V add_leaf_points(const DevTree& t, int4 tc, float3 q,
+                                                         const KParams& kp, typename A::V acc) {
   for (int i = tc.z; i < tc.w; i++)
-    acc = radd(acc, kernel_exact<DIM, K>(__ldg(t.pt_pm + i), __ldg(t.pt_nrm + i), q, kp));
+    acc = A::add(acc, A::point(__ldg(t.pt_pm + i), __ldg(t.pt_nrm + i), q, kp));
   return acc;
 }
 
@@ -146,10 +149,11 @@ __device__ __forceinline__ float add_leaf_points(const DevTree& t, int4 tc, floa
 // kv = k(v) and the children sum sum_{children c} k(c) in cell order, leaf
 // children point by point (include/tree_sampler.h:264-280), and `contribs`, the
 // number of kernel evaluations that sum stands for.  All lanes must call.
-template <int DIM, int K>
-__device__ __forceinline__ float expand(const DevTree& t, bool own, int v, int4 tv, float3 q,
-                                        const KParams& kp, const ExpandSmem& sm, int lane,
-                                        float& kv, int& contribs) {
+template <class A>
+__device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int v, int4 tv,
+                                                float3 q, const KParams& kp,
+                                                const ExpandSmem<typename A::V>& sm, int lane,
+                                                typename A::V& kv, int& contribs) {
   const int nent = own ? tv.y + 1 : 0;
   int incl = nent;
 #pragma unroll
@@ -159,8 +163,8 @@ __device__ __forceinline__ float expand(const DevTree& t, bool own, int v, int4 
   }
   const int excl = incl - nent;
   const int total = __shfl_sync(0xffffffffu, incl, 31);
-  float acc = 0.f;
-  kv = 0.f;
+  typename A::V acc = A::zero();
+  kv = A::zero();
   contribs = 0;
   for (int base = 0; base < total; base += SBH_VCAP) {
     const int end = min(total, base + SBH_VCAP);
@@ -174,7 +178,7 @@ __device__ __forceinline__ float expand(const DevTree& t, bool own, int v, int4 
       const int4 tc = __ldg(t.nd_topo + c);
       const float4 cm = __ldg(t.nd_cm + c), ag = __ldg(t.nd_agg + c);
       if (tc.y == 0 && tc.w - tc.z != 1) atomicOr(sm.multi + (r >> 5), 1u << (r & 31));
-      sm.vals[r] = kernel_node<DIM, K>(cm, ag, q, kp);
+      sm.vals[r] = A::node(cm, ag, q, kp);
     }
     __syncwarp();
     for (int p = s0; p < s1; p++) {
@@ -183,10 +187,10 @@ __device__ __forceinline__ float expand(const DevTree& t, bool own, int v, int4 
         kv = sm.vals[r];
       } else if ((sm.multi[r >> 5] >> (r & 31)) & 1u) {
         const int4 tc = __ldg(t.nd_topo + tv.x + (p - excl - 1));
-        acc = add_leaf_points<DIM, K>(t, tc, q, kp, acc);
+        acc = add_leaf_points<A>(t, tc, q, kp, acc);
         contribs += tc.w - tc.z;
       } else {
-        acc = radd(acc, sm.vals[r]);
+        acc = A::add(acc, sm.vals[r]);
         contribs += 1;
       }
     }
@@ -230,25 +234,29 @@ __device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 
 }
 
 
-// Shared-memory scratch of one warp running the sampler (sbh_warp_words floats).
+// Shared-memory scratch of one warp running the sampler (sbh_warp_words<V>
+// 4-byte words; V is the policy's value).
+template <class V>
 struct SbhWarpSmem {
-  float* bhS;     // [R] BH term of each subdomain
-  float* diffS;   // [R] first-step difference of each subdomain
+  V* bhS;         // [R] BH term of each subdomain
+  V* diffS;       // [R] first-step difference of each subdomain
   int* ccS;       // [R] contributions of that difference
-  float* pathv;   // [32] per-path corrections of the current round
-  ExpandSmem ex;
+  V* pathv;       // [32] per-path corrections of the current round
+  ExpandSmem<V> ex;
 };
 
+template <class V>
 __host__ __device__ constexpr int sbh_warp_words(int R) {
-  return 3 * R + 32 + 2 * SBH_VCAP + SBH_VCAP / 32;
+  return (int)(sizeof(V) / 4) * (2 * R + 32 + SBH_VCAP) + R + SBH_VCAP + SBH_VCAP / 32;
 }
 
-__device__ __forceinline__ SbhWarpSmem sbh_carve(float* base, int R) {
-  SbhWarpSmem w;
-  w.bhS = base;
-  w.diffS = base + R;
-  w.ccS = reinterpret_cast<int*>(base + 2 * R);
-  w.pathv = base + 3 * R;
+template <class V>
+__device__ __forceinline__ SbhWarpSmem<V> sbh_carve(float* base, int R) {
+  SbhWarpSmem<V> w;
+  w.bhS = reinterpret_cast<V*>(base);
+  w.diffS = w.bhS + R;
+  w.ccS = reinterpret_cast<int*>(w.diffS + R);
+  w.pathv = reinterpret_cast<V*>(w.ccS + R);
   w.ex.vals = w.pathv + 32;
   w.ex.ent = reinterpret_cast<int*>(w.ex.vals + SBH_VCAP);
   w.ex.multi = reinterpret_cast<unsigned*>(w.ex.ent + SBH_VCAP);
@@ -257,22 +265,25 @@ __device__ __forceinline__ SbhWarpSmem sbh_carve(float* base, int R) {
 
 // The whole estimator for one query, one warp: see sampler.cu for the method.
 // qi is the query's index in its request (it keys the Philox streams).  The
-// result and its contribution count are returned on lane 0.
-template <int DIM, int K>
+// result and its contribution count are returned on lane 0.  Sums follow the
+// policy A; the sampled paths depend only on the tree, the query and the
+// random streams, so every policy walks the same paths for the same seed.
+template <int DIM, int K, class A = SumF<DIM, K>>
 __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long qi, int samples,
                                           unsigned long long seed, const KParams& kp,
-                                          const SbhWarpSmem& ws, int* status, float& result,
-                                          int& count) {
+                                          const SbhWarpSmem<typename A::V>& ws, int* status,
+                                          typename A::V& result, int& count) {
+  using V = typename A::V;
   const int lane = threadIdx.x & 31;
   const int R = t.root_children;
   const float inf = __int_as_float(0x7f800000);
   const int c0 = __ldg(t.nd_topo).x;
-  result = 0.f;
+  result = A::zero();
   count = 0;
   if (R == 0) return;  // a single-leaf tree has no subdomains (tree_sampler.h:214)
   int cnt = 0;
 
-  // Phase A: BH term and first-step difference of every subdomain.
+// Phase A: BH term and first-step difference of every subdomain.
   for (int g = 0; g < R; g += 32) {
     const int j = g + lane;
     const bool have = j < R;
@@ -284,11 +295,11 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     }
     const bool own = have && tS.y != 0;
     int cc;
-    float kS;
-    const float sumc = expand<DIM, K>(t, own, c0 + j, tS, q, kp, ws.ex, lane, kS, cc);
+    V kS;
+    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, ws.ex, lane, kS, cc);
     if (have) {
       ws.bhS[j] = kS;
-      ws.diffS[j] = own ? rsub(sumc, kS) : 0.f;
+      ws.diffS[j] = own ? A::sub(sumc, kS) : A::zero();
       ws.ccS[j] = cc;
     }
   }
@@ -296,11 +307,11 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
 
   // Phase B: sampled paths, 32 at a time, advanced step by step in lock step.
   const int P = R * samples;
-  float mlcv = 0.f, sub = 0.f;
+  V mlcv = A::zero(), sub = A::zero();
   int cur_sub = -1;
   for (int pbase = 0; pbase < P; pbase += 32) {
     const int pid = pbase + lane;
-    float wd = 0.f;
+    V wd = A::zero();
     bool active = false;
     int j = 0, S = 0, cur = 0;
     int4 tcur = make_int4(0, 0, 0, 0);
@@ -344,13 +355,13 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
           cur = contained_in_child<DIM>(t, prev, tprev, p, tnext);
           if (cur < 0) {
             report_status(status, kStatusNullChild);
-            wd = __int_as_float(0x7fc00000);
+            wd = A::nan();
             active = false;
           } else {
             cb = (cb < ffr) ? ffr : cb;
             w = rdiv(spi, rmul(ev, (float)(unsigned)(tprev.w - tprev.z)));
             if (prev == S) {
-              wd = radd(wd, rmul(w, ws.diffS[j]));
+              wd = A::add(wd, A::scale(w, ws.diffS[j]));
               cnt += ws.ccS[j];
             } else {
               own = true;
@@ -361,10 +372,10 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
         }
       }
       int cc;
-      float kprev;
-      const float sumc = expand<DIM, K>(t, own, prev, tprev, q, kp, ws.ex, lane, kprev, cc);
+      V kprev;
+      const V sumc = expand<A>(t, own, prev, tprev, q, kp, ws.ex, lane, kprev, cc);
       if (own) {
-        wd = radd(wd, rmul(w, rsub(sumc, kprev)));
+        wd = A::add(wd, A::scale(w, A::sub(sumc, kprev)));
         cnt += cc;
       }
     }
@@ -375,11 +386,11 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       for (int k = 0; k < m; k++) {
         const int jj = (pbase + k) / samples;
         if (jj != cur_sub) {
-          if (cur_sub >= 0) mlcv = radd(mlcv, rdiv(sub, (float)samples));
-          sub = 0.f;
+          if (cur_sub >= 0) mlcv = A::add(mlcv, A::div(sub, (float)samples));
+          sub = A::zero();
           cur_sub = jj;
         }
-        sub = radd(sub, ws.pathv[k]);
+        sub = A::add(sub, ws.pathv[k]);
       }
     }
     __syncwarp();
@@ -388,17 +399,17 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if (lane == 0) {
-    if (cur_sub >= 0) mlcv = radd(mlcv, rdiv(sub, (float)samples));
-    float bh = 0.f;
+    if (cur_sub >= 0) mlcv = A::add(mlcv, A::div(sub, (float)samples));
+    V bh = A::zero();
     for (int j = 0; j < R; j++) {
       const int4 tS = __ldg(t.nd_topo + c0 + j);
       if (tS.y == 0) {
-        bh = add_leaf_points<DIM, K>(t, tS, q, kp, bh);
+        bh = add_leaf_points<A>(t, tS, q, kp, bh);
       } else {
-        bh = radd(bh, ws.bhS[j]);
+        bh = A::add(bh, ws.bhS[j]);
       }
     }
-    result = radd(bh, mlcv);
+    result = A::add(bh, mlcv);
     count = cnt;
   }
   __syncwarp();  // the next query of this warp overwrites the scratch

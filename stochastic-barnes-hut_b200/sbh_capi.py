@@ -61,6 +61,8 @@ _SIGNATURES = {
     "sbh_server_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_double, _P]),
     "sbh_server_stats_get": (ctypes.c_int, [_P, _P]),
     "sbh_server_destroy": (None, [_P]),
+    "sbh_eval_grad": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _P]),
+    "sbh_eval_grad_device": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P]),
 }
 
 # Largest query count sbh_eval_device_static_scratch accepts per call.
@@ -217,6 +219,7 @@ class GpuTree:
         _check(lib().sbh_gpu_tree_info(h, ctypes.byref(i)))
         self.info = i
         self.dim = i.dim
+        self.device = device
 
     def eval(self, queries, p: Params, stream: int = 0, contribs: bool = False):
         """Blocking evaluation of host queries (n, dim): returns (values, kernel_ms[, counts])."""
@@ -256,6 +259,32 @@ class GpuTree:
             self.handle, ctypes.byref(p), ctypes.c_void_p(d_queries), nq,
             ctypes.c_void_p(d_results), ctypes.c_void_p(d_contribs or None),
             ctypes.c_void_p(stream)))
+
+    def eval_grad(self, queries, p: Params, stream: int = 0, contribs: bool = False,
+                  grads: bool = True):
+        """Blocking sbh_eval_grad of host queries (n, dim): returns (values, grads
+        (n, dim) or None, kernel_ms[, counts])."""
+        q = np.asfortranarray(queries, np.float32)
+        if q.ndim != 2 or q.shape[1] != self.dim:
+            raise ValueError(f"queries must be (n, {self.dim})")
+        nq = q.shape[0]
+        out = np.zeros(nq, np.float32)
+        g = np.zeros((nq, self.dim), np.float32, order="F") if grads else None
+        cnt = np.zeros(nq, np.int32) if contribs else None
+        ms = ctypes.c_float(0)
+        _check(lib().sbh_eval_grad(self.handle, ctypes.byref(p), _ptr(q), nq, _ptr(out), _ptr(g),
+                                   _ptr(cnt), ctypes.byref(ms), ctypes.c_void_p(stream)))
+        return (out, g, ms.value, cnt) if contribs else (out, g, ms.value)
+
+    def eval_grad_device(self, d_queries: int, nq: int, d_values: int, d_grads: int, p: Params,
+                         stream: int = 0, d_contribs: int = 0):
+        """Asynchronous sbh_eval_grad_device on device pointers (SoA queries and
+        gradients [dim][nq] float32; d_grads may be 0)."""
+        _check(lib().sbh_eval_grad_device(self.handle, ctypes.byref(p), ctypes.c_void_p(d_queries),
+                                          nq, ctypes.c_void_p(d_values),
+                                          ctypes.c_void_p(d_grads or None),
+                                          ctypes.c_void_p(d_contribs or None),
+                                          ctypes.c_void_p(stream)))
 
     def check(self, stream: int = 0):
         _check(lib().sbh_gpu_tree_check(self.handle, ctypes.c_void_p(stream)))
