@@ -285,6 +285,24 @@ def run_ours(args, wl):
     kmean_s = statistics.mean(kern_ms) / 1e3
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / kmean_s / 1e9
+    if wl["method"] == "brute_force":
+        # Brute force is bound by the MUFU pipe: one rsqrt per Plummer pair (two
+        # MUFU ops -- rsqrt and reciprocal -- for gravity and the winding number).
+        rates = C.measure_pipe_rates(local)
+        mufu_per_pair = 1 if wl["kernel"] == "plummer" else 2
+        pairs = float(nq) * float(wl["n"])
+        roofline = {
+            "bound": "sfu", "kernel": "brute_force_kernel",
+            "achieved": pairs / kmean_s, "peak": rates["rsqrt_per_s"] / mufu_per_pair,
+            "unit": "pairs/s", "frac": pairs / kmean_s / (rates["rsqrt_per_s"] / mufu_per_pair),
+            "peak_source": "measured MUFU rsqrt rate (sbh_measure_pipe_rates): "
+                           f"{rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
+                           f"{rates['sm_clock_mhz']:.0f} MHz; {mufu_per_pair} MUFU op(s) per pair",
+            "kernel_ms": statistics.mean(kern_ms), "pairs_per_launch": pairs,
+            "pipe_rates": rates, "traffic": None,
+        }
+    else:
+        roofline = None
     launches_per_step = {"stochastic": 6, "barnes_hut": 6, "brute_force": 1}[wl["method"]]
     clk = clocks.summary()
     out = {
@@ -316,7 +334,7 @@ def run_ours(args, wl):
         "e2e": {"value": world * nq / (e2e_ms / 1e3 / args.steps), "unit": "queries/s",
                 "h2d_bytes_per_step": nq * 12, "d2h_bytes_per_step": nq * 4,
                 "ms_per_step": e2e_ms / args.steps},
-        "roofline": {
+        "roofline": roofline or {
             "bound": "hbm", "kernel": "stochastic_kernel" if wl["method"] == "stochastic" else wl["method"],
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",

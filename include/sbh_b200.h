@@ -289,6 +289,15 @@ int sbh_eval_grad_device(sbh_gpu_tree* tree, const sbh_params* params, const flo
                          int64_t nq, float* d_values, float* d_grads, int32_t* d_contribs,
                          void* stream);
 
+/* ---- diagnostics ---------------------------------------------------------------
+ * No counterpart in the reference.  Measures on `device` the throughput of the
+ * arithmetic the brute-force kernel is bound by: MUFU reciprocal square roots,
+ * scalar FP32 FMAs and packed FP32x2 FMA lanes, per second, plus rsqrt per clock
+ * per SM and the SM clock the loops ran at (about 0.1 s of GPU time). */
+int sbh_measure_pipe_rates(int device, double* rsqrt_per_s, double* ffma_per_s,
+                           double* ffma2_lanes_per_s, double* rsqrt_per_clk_sm,
+                           double* sm_clock_mhz);
+
 #ifdef __cplusplus
 }
 #endif

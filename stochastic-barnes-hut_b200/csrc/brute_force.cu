@@ -2,18 +2,23 @@
 // include/brute_force_gpu.h:18-66, and its wrappers src/sbh_gpu.cu:39-77).
 //
 // Design (B200):
-//   * A cluster of C CTAs owns one tile of BF_THREADS*QPT queries; CTA rank r
+//   * A cluster of C CTAs owns one tile of THREADS*BF_QPT queries; CTA rank r
 //     sums source chunk r of C.  The C partial sums of a query are combined in
 //     rank order through distributed shared memory, so there is no global
 //     scratch buffer and no second launch, and results are deterministic.
-//   * Sources are staged in shared memory tiles of float4 (x, y, z, m) (plus a
-//     float4 normal tile for the winding number); every lane of a warp reads the
-//     same source, a broadcast.
-//   * Each thread carries QPT queries; the inner loop is FMA plus one MUFU
-//     rsqrt per pair for the Plummer and gravity potentials.
+//   * Each thread carries BF_QPT = 8 queries as four pairs, and the pairwise
+//     arithmetic runs on Blackwell's packed FP32 instructions (FADD2 / FMUL2 /
+//     FFMA2, two lanes of FP32 per issue): a Plummer pair costs 3.5 FP32 issue
+//     slots plus one MUFU rsqrt, so the kernel is bound by the MUFU pipe (16
+//     results per clock per SM), not by issue.
+//   * Sources are staged in shared memory with every coordinate duplicated into
+//     both halves of a float2 (x,x | y,y | z,z | m,m), so one broadcast
+//     shared load gives the packed operand directly.
 //   * Compensated accumulation in two levels: plain FP32 over BF_SUB sources,
 //     then a Knuth two-sum into a (sum, error) pair -- the reference's Kahan
-//     loop (brute_force_gpu.h:52-60) at a ~1/BF_SUB of its cost per pair.
+//     loop (brute_force_gpu.h:52-60) at ~1/BF_SUB of its cost per pair.
+//   * Grid shape: the launcher picks the CTA size (64 or 128 threads) and the
+//     cluster size (1-8) that spread the CTAs most evenly over the SMs.
 #include <cooperative_groups.h>
 
 #include "launch.h"
@@ -24,33 +29,117 @@ namespace cg = cooperative_groups;
 namespace sbh {
 namespace {
 
-constexpr int BF_THREADS = 128;
-constexpr int BF_QPT = 4;
-constexpr int BF_TILE = 512;
-constexpr int BF_SUB = 64;
-constexpr int BF_QUERIES_PER_CTA = BF_THREADS * BF_QPT;
+constexpr int BF_QPT = 8;                 // queries per thread
+constexpr int BF_PAIRS = BF_QPT / 2;      // packed query pairs per thread
+constexpr int BF_TILE = 512;              // sources per shared-memory stage
+constexpr int BF_SUB = 64;                // sources per plain partial sum
 
+// One source duplicated into both lanes of float2 pairs.
+struct __align__(16) SrcPair {
+  float2 x, y, z, m;
+};
+struct __align__(16) NrmPair {
+  float2 x, y, z, unused;
+};
+
+__device__ __forceinline__ float2 dup(float v) { return make_float2(v, v); }
+
+// One MUFU operation each, denormal inputs and results flushed to zero (the
+// PTX approximate instructions; the non-ftz library forms add FP32-pipe work
+// to every pair for denormal scaling, and the FP32 pipe is nearly as loaded as
+// the MUFU here).  Relative error of both is below 2^-22.
+__device__ __forceinline__ float mufu_rsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float mufu_rcp(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float2 rsqrt2(float2 x) {
+  return make_float2(mufu_rsqrt(x.x), mufu_rsqrt(x.y));
+}
+__device__ __forceinline__ float2 rcp2(float2 x) { return make_float2(mufu_rcp(x.x), mufu_rcp(x.y)); }
+
+// r = |d| from r^2, per lane: r2 * rsqrt(r2).  Below the normal range (which
+// the rsqrt flushes to zero) r is taken as 0.
+__device__ __forceinline__ float2 norm_from_sq(float2 r2) {
+  const float2 r = __fmul2_rn(r2, rsqrt2(r2));
+  return make_float2(r2.x >= 1.17549435e-38f ? r.x : 0.f, r2.y >= 1.17549435e-38f ? r.y : 0.f);
+}
+
+// part += kernel values of source s at the query pair (-nq = negated queries).
+// Same functions as kernel_fast (tasks.cuh), two queries per instruction.
+// Gravity accumulates +m / (r + 0.1); the caller negates the total.
 template <int DIM, int K>
-__global__ void __launch_bounds__(BF_THREADS) brute_force_kernel(DevTree t,
-                                                                 const float* __restrict__ qsoa,
-                                                                 long long nq, KParams kp,
-                                                                 float* __restrict__ out) {
+__device__ __forceinline__ float2 accumulate2(float2 part, const SrcPair& s, const NrmPair& n,
+                                              float2 nqx, float2 nqy, float2 nqz,
+                                              const KParams& kp) {
+  const float2 dx = __fadd2_rn(s.x, nqx);
+  const float2 dy = __fadd2_rn(s.y, nqy);
+  const float2 dz = DIM == 3 ? __fadd2_rn(s.z, nqz) : make_float2(0.f, 0.f);
+  if (K == kPlummer) {
+    float2 r2 = __ffma2_rn(dx, dx, dup(kp.eps2));
+    r2 = __ffma2_rn(dy, dy, r2);
+    if (DIM == 3) r2 = __ffma2_rn(dz, dz, r2);
+    return __ffma2_rn(s.m, rsqrt2(r2), part);
+  }
+  float2 r2 = __fmul2_rn(dx, dx);
+  r2 = __ffma2_rn(dy, dy, r2);
+  if (DIM == 3) r2 = __ffma2_rn(dz, dz, r2);
+  if (K == kGravity) {
+    const float2 den = __fadd2_rn(norm_from_sq(r2), dup(1e-1f));
+    return __ffma2_rn(s.m, rcp2(den), part);
+  } else if (K == kWindingNumber) {
+    float2 qdn = __fmul2_rn(n.x, dx);
+    qdn = __ffma2_rn(n.y, dy, qdn);
+    if (DIM == 3) qdn = __ffma2_rn(n.z, dz, qdn);
+    const float2 num = __fmul2_rn(s.m, qdn);
+    float2 den;
+    if (DIM == 2) {
+      den = __fmul2_rn(dup(kTwoPi), __fadd2_rn(r2, dup(1e-5f)));
+    } else {
+      den = __fmul2_rn(dup(kFourPi), __ffma2_rn(r2, norm_from_sq(r2), dup(1e-5f)));
+    }
+    return __ffma2_rn(num, rcp2(den), part);
+  } else {  // smooth distance
+    const float2 t = __fmul2_rn(dup(-kp.alpha), norm_from_sq(r2));
+    return __fadd2_rn(part, make_float2(expf(t.x), expf(t.y)));
+  }
+}
+
+template <int THREADS, int DIM, int K>
+__global__ void __launch_bounds__(THREADS) brute_force_kernel(DevTree t,
+                                                              const float* __restrict__ qsoa,
+                                                              long long nq, KParams kp,
+                                                              float* __restrict__ out) {
   constexpr bool kNormals = (K == kWindingNumber);
-  __shared__ float4 s_pm[BF_TILE];
-  __shared__ float4 s_nr[kNormals ? BF_TILE : 1];
-  __shared__ float2 s_part[BF_QUERIES_PER_CTA];
+  constexpr int kQueriesPerCta = THREADS * BF_QPT;
+  __shared__ SrcPair s_src[BF_TILE];
+  __shared__ NrmPair s_nrm[kNormals ? BF_TILE : 1];
+  __shared__ float2 s_part[kQueriesPerCta];
 
   cg::cluster_group cluster = cg::this_cluster();
   const int csize = (int)cluster.num_blocks();
   const int rank = (int)cluster.block_rank();
   const long long tile = blockIdx.x / csize;
-  const long long q0 = tile * BF_QUERIES_PER_CTA;
+  const long long q0 = tile * kQueriesPerCta;
 
-  float3 q[BF_QPT];
+  // Query j of this thread is q0 + threadIdx.x + j * THREADS; pair p holds
+  // queries 2p and 2p+1, negated so the differences are packed adds.
+  float2 nqx[BF_PAIRS], nqy[BF_PAIRS], nqz[BF_PAIRS];
 #pragma unroll
-  for (int j = 0; j < BF_QPT; j++) {
-    const long long qi = q0 + threadIdx.x + j * BF_THREADS;
-    q[j] = qi < nq ? load_query<DIM>(qsoa, nq, qi) : make_float3(0.f, 0.f, 0.f);
+  for (int p = 0; p < BF_PAIRS; p++) {
+    float3 a = make_float3(0.f, 0.f, 0.f), b = a;
+    const long long qa = q0 + threadIdx.x + (2 * p) * THREADS;
+    const long long qb = qa + THREADS;
+    if (qa < nq) a = load_query<DIM>(qsoa, nq, qa);
+    if (qb < nq) b = load_query<DIM>(qsoa, nq, qb);
+    nqx[p] = make_float2(-a.x, -b.x);
+    nqy[p] = make_float2(-a.y, -b.y);
+    nqz[p] = make_float2(-a.z, -b.z);
   }
   float hi[BF_QPT], lo[BF_QPT];
 #pragma unroll
@@ -59,76 +148,82 @@ __global__ void __launch_bounds__(BF_THREADS) brute_force_kernel(DevTree t,
   const long long chunk = (t.n + csize - 1) / csize;
   const long long c0 = min((long long)rank * chunk, t.n);
   const long long c1 = min(c0 + chunk, t.n);
+  const NrmPair no_normal = {};
 
   for (long long base = c0; base < c1; base += BF_TILE) {
     const int len = (int)min((long long)BF_TILE, c1 - base);
-    for (int k = threadIdx.x; k < len; k += BF_THREADS) {
-      s_pm[k] = __ldg(t.pt_pm + base + k);
-      if (kNormals) s_nr[k] = __ldg(t.pt_nrm + base + k);
+    for (int k = threadIdx.x; k < len; k += THREADS) {
+      const float4 v = __ldg(t.pt_pm + base + k);
+      s_src[k] = SrcPair{dup(v.x), dup(v.y), dup(v.z), dup(v.w)};
+      if (kNormals) {
+        const float4 n = __ldg(t.pt_nrm + base + k);
+        s_nrm[k] = NrmPair{dup(n.x), dup(n.y), dup(n.z), dup(0.f)};
+      }
     }
     __syncthreads();
     for (int sb = 0; sb < len; sb += BF_SUB) {
       const int se = min(sb + BF_SUB, len);
-      float part[BF_QPT];
+      float2 part[BF_PAIRS];
 #pragma unroll
-      for (int j = 0; j < BF_QPT; j++) part[j] = 0.f;
+      for (int p = 0; p < BF_PAIRS; p++) part[p] = make_float2(0.f, 0.f);
       if (se - sb == BF_SUB) {
-#pragma unroll 8
+#pragma unroll 4
         for (int k = sb; k < sb + BF_SUB; k++) {
-          const float4 s = s_pm[k];
-          const float4 nr = kNormals ? s_nr[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+          const SrcPair sp = s_src[k];
+          const NrmPair np = kNormals ? s_nrm[k] : no_normal;
 #pragma unroll
-          for (int j = 0; j < BF_QPT; j++) part[j] += kernel_fast<DIM, K>(s, nr, q[j], kp);
+          for (int p = 0; p < BF_PAIRS; p++)
+            part[p] = accumulate2<DIM, K>(part[p], sp, np, nqx[p], nqy[p], nqz[p], kp);
         }
       } else {
         for (int k = sb; k < se; k++) {
-          const float4 s = s_pm[k];
-          const float4 nr = kNormals ? s_nr[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+          const SrcPair sp = s_src[k];
+          const NrmPair np = kNormals ? s_nrm[k] : no_normal;
 #pragma unroll
-          for (int j = 0; j < BF_QPT; j++) part[j] += kernel_fast<DIM, K>(s, nr, q[j], kp);
+          for (int p = 0; p < BF_PAIRS; p++)
+            part[p] = accumulate2<DIM, K>(part[p], sp, np, nqx[p], nqy[p], nqz[p], kp);
         }
       }
 #pragma unroll
-      for (int j = 0; j < BF_QPT; j++) two_sum_add(hi[j], lo[j], part[j]);
+      for (int p = 0; p < BF_PAIRS; p++) {
+        two_sum_add(hi[2 * p], lo[2 * p], part[p].x);
+        two_sum_add(hi[2 * p + 1], lo[2 * p + 1], part[p].y);
+      }
     }
     __syncthreads();
   }
 
 #pragma unroll
-  for (int j = 0; j < BF_QPT; j++) s_part[threadIdx.x + j * BF_THREADS] = make_float2(hi[j], lo[j]);
+  for (int j = 0; j < BF_QPT; j++) s_part[threadIdx.x + j * THREADS] = make_float2(hi[j], lo[j]);
   cluster.sync();
   if (rank == 0) {
     for (int r = 1; r < csize; r++) {
       const float2* peer = cluster.map_shared_rank(s_part, r);
 #pragma unroll
       for (int j = 0; j < BF_QPT; j++) {
-        const float2 v = peer[threadIdx.x + j * BF_THREADS];
+        const float2 v = peer[threadIdx.x + j * THREADS];
         two_sum_add(hi[j], lo[j], v.x);
         lo[j] += v.y;
       }
     }
 #pragma unroll
     for (int j = 0; j < BF_QPT; j++) {
-      const long long qi = q0 + threadIdx.x + j * BF_THREADS;
-      if (qi < nq) out[qi] = hi[j] + lo[j];
+      const long long qi = q0 + threadIdx.x + j * THREADS;
+      const float v = hi[j] + lo[j];
+      if (qi < nq) out[qi] = K == kGravity ? -v : v;
     }
   }
   // Peers keep their shared memory alive until rank 0 has read it.
   cluster.sync();
 }
 
-template <int DIM, int K>
-cudaError_t launch_bf(const DevTree& t, const float* q, long long nq, const KParams& kp, float* out,
-                      cudaStream_t stream, int sm_count) {
-  const long long tiles = (nq + BF_QUERIES_PER_CTA - 1) / BF_QUERIES_PER_CTA;
-  // Split sources over up to 8 CTAs per cluster until the grid covers the
-  // GPU several times over; never split below one source tile per CTA.
-  int csize = 1;
-  while (csize < 8 && tiles * csize < 4LL * sm_count && t.n >= (long long)BF_TILE * csize * 2)
-    csize *= 2;
+template <int THREADS, int DIM, int K>
+cudaError_t launch_bf_shape(const DevTree& t, const float* q, long long nq, const KParams& kp,
+                            float* out, cudaStream_t stream, int csize) {
+  const long long tiles = (nq + THREADS * BF_QPT - 1) / (THREADS * BF_QPT);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(tiles * csize), 1, 1);
-  cfg.blockDim = dim3(BF_THREADS, 1, 1);
+  cfg.blockDim = dim3(THREADS, 1, 1);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
@@ -138,7 +233,36 @@ cudaError_t launch_bf(const DevTree& t, const float* q, long long nq, const KPar
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, brute_force_kernel<DIM, K>, t, q, nq, kp, out);
+  return cudaLaunchKernelEx(&cfg, brute_force_kernel<THREADS, DIM, K>, t, q, nq, kp, out);
+}
+
+template <int DIM, int K>
+cudaError_t launch_bf(const DevTree& t, const float* q, long long nq, const KParams& kp, float* out,
+                      cudaStream_t stream, int sm_count) {
+  // Every CTA does the same work (THREADS * BF_QPT queries x n / csize
+  // sources) and the kernel is bound per SM, so the run takes about
+  // ceil(CTAs / SMs) CTA-times.  Pick the shape with the least of that time,
+  // preferring fewer clusters (less reduction) on ties; never split sources
+  // below two stages per CTA.
+  int best_threads = 128, best_c = 1;
+  double best = -1.0;
+  for (int threads : {128, 64}) {
+    const long long tiles = (nq + threads * BF_QPT - 1) / (threads * BF_QPT);
+    for (int c = 1; c <= 8; c *= 2) {
+      if (c > 1 && t.n < (long long)BF_TILE * c * 2) break;
+      const long long ctas = tiles * c;
+      const double waves = (double)((ctas + sm_count - 1) / sm_count);
+      const double cost = waves * threads / c;
+      if (best < 0.0 || cost < best * 0.999) {
+        best = cost;
+        best_threads = threads;
+        best_c = c;
+      }
+    }
+  }
+  if (best_threads == 128)
+    return launch_bf_shape<128, DIM, K>(t, q, nq, kp, out, stream, best_c);
+  return launch_bf_shape<64, DIM, K>(t, q, nq, kp, out, stream, best_c);
 }
 
 }  // namespace

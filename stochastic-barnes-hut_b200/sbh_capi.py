@@ -63,6 +63,7 @@ _SIGNATURES = {
     "sbh_server_destroy": (None, [_P]),
     "sbh_eval_grad": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _P]),
     "sbh_eval_grad_device": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P]),
+    "sbh_measure_pipe_rates": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P]),
 }
 
 # Largest query count sbh_eval_device_static_scratch accepts per call.
@@ -311,6 +312,15 @@ def eval_batch(entries, stream: int = 0):
         arr[i].d_contribs = dcnt or None
         arr[i].d_self_mass = dself or None
     _check(lib().sbh_eval_batch(arr, len(entries), ctypes.c_void_p(stream)))
+
+
+def measure_pipe_rates(device: int = 0) -> dict:
+    """sbh_measure_pipe_rates: measured MUFU rsqrt / FFMA / FFMA2-lane rates."""
+    v = [ctypes.c_double(0) for _ in range(5)]
+    _check(lib().sbh_measure_pipe_rates(device, *[ctypes.byref(x) for x in v]))
+    return {"rsqrt_per_s": v[0].value, "ffma_per_s": v[1].value,
+            "ffma2_lanes_per_s": v[2].value, "rsqrt_per_clk_sm": v[3].value,
+            "sm_clock_mhz": v[4].value}
 
 
 class Request:
