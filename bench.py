@@ -97,55 +97,117 @@ def method_id(C, name):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 2 ms from a thread (read-only queries), or
+    nvidia-smi at 100 ms where NVML is unavailable."""
 
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index: int):
-        self.rows = []
-        self.proc = None
         self.dev = device_index
+        self.sm, self.sm_max, self.reasons = [], [], set()
+        self.proc = None
+        self.thread = None
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        """NVML handle of CUDA device `dev`: the NVML device whose PCI domain,
+        bus and device numbers equal the CUDA device's (NVML enumerates every
+        GPU of the machine, CUDA only the visible ones).  Only NVML handles and
+        integers are passed to NVML."""
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.dev)
+        want = (int(props.pci_domain_id), int(props.pci_bus_id), int(props.pci_device_id))
+        for i in range(pynvml.nvmlDeviceGetCount()):
+            h = pynvml.nvmlDeviceGetHandleByIndex(i)
+            pci = pynvml.nvmlDeviceGetPciInfo(h)
+            if (int(pci.domain), int(pci.bus), int(pci.device)) == want:
+                return pynvml, h
+        raise RuntimeError("no NVML device matches the CUDA device")
+
+    def _poll_nvml(self, nv, h):
+        masks = [(name, getattr(nv, attr)) for name, attr in self.REASONS]
+        while not self.stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                self.sm_max.append(float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.reasons.update(name for name, m in masks if r & m)
+            except Exception:
+                break
+            self.stop.wait(0.002)
+
+    def _read_smi(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) != 9:
+                continue
+            if parts[1].replace(".", "").isdigit():
+                self.sm.append(float(parts[1]))
+            if parts[2].replace(".", "").isdigit():
+                self.sm_max.append(float(parts[2]))
+            self.reasons.update(self.REASONS[i][0] for i in range(4)
+                                if parts[5 + i].lower() == "active")
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100", "-i", str(self.dev)], stdout=subprocess.PIPE,
-                stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+            nv, h = self._nvml_handle()
+            self.thread = threading.Thread(target=self._poll_nvml, args=(nv, h), daemon=True)
         except Exception:
-            self.proc = None
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                     "-lms", "100", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                    stderr=subprocess.DEVNULL, text=True)
+                self.thread = threading.Thread(target=self._read_smi, daemon=True)
+            except Exception:
+                self.thread = None
+        if self.thread:
+            self.thread.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) == 9:
-                self.rows.append(parts)
-
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread:
             self.thread.join(timeout=2)
 
     def summary(self):
-        if not self.rows:
+        if not self.sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4)
-                          if r[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+        return {"sm_mhz": statistics.median(self.sm),
+                "sm_max_mhz": max(self.sm_max) if self.sm_max else None,
+                "reasons": sorted(self.reasons), "samples": len(self.sm)}
+
+
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of each rank's timings, returned on every rank (the
+    job's time is its slowest rank's).  `dist` is torch.distributed with a
+    process group initialised, or None for a single process."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def whole_job_rate(world, units_per_rank, total_ms, steps):
+    """Units all ranks processed per second, over the slowest rank's time."""
+    return world * units_per_rank / (total_ms / 1e3 / steps)
 
 
 def dist_setup():
@@ -273,9 +335,7 @@ def run_ours(args, wl):
                                             s_handle, args)
 
     if dist:
-        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_ms = t.tolist()
+        total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dist, dev)
         dist.destroy_process_group()
     if rank != 0:
         return None
@@ -307,7 +367,7 @@ def run_ours(args, wl):
     clk = clocks.summary()
     out = {
         "metric": METRIC,
-        "value": world * nq / (total_ms / 1e3 / args.steps),
+        "value": whole_job_rate(world, nq, total_ms, args.steps),
         "unit": "queries/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -331,7 +391,7 @@ def run_ours(args, wl):
             "l2": "512 MiB buffer written between timed steps; tree+queries exceed L2 as well",
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         },
-        "e2e": {"value": world * nq / (e2e_ms / 1e3 / args.steps), "unit": "queries/s",
+        "e2e": {"value": whole_job_rate(world, nq, e2e_ms, args.steps), "unit": "queries/s",
                 "h2d_bytes_per_step": nq * 12, "d2h_bytes_per_step": nq * 4,
                 "ms_per_step": e2e_ms / args.steps},
         "roofline": roofline or {
@@ -669,6 +729,8 @@ def run_serving(args):
     results = {"plain_bh_capacity": {"queries_per_s": total_q / mk, "requests_per_s": plain_rps,
                                      "median_rel_err": serving_errors(C, trees, reqs, gpus,
                                                                       plain_outs, pick)}}
+    sampler = ClockSampler(0)
+    sampler.__enter__()
     for factor in (0.5, 1.0, 2.0, 8.0):
         rate = factor * plain_rps
         gaps = rng.exponential(1.0 / rate, len(reqs))
@@ -685,6 +747,7 @@ def run_serving(args):
             if factor == 8.0:
                 row[name]["median_rel_err"] = serving_errors(C, trees, reqs, gpus, outs, pick)
         results[f"rate_x{factor}"] = row
+    sampler.__exit__(None, None, None)
     stats = server.stats()
     server.close()
     hi = results["rate_x8.0"]
@@ -699,7 +762,7 @@ def run_serving(args):
                                "plain per-call BH (theta 0.5)",
                    "requests": len(reqs), "queries": total_q, "setup_s": setup_s,
                    "server": {"slots": 3, "slot_queries": 1 << 20}},
-        "serving": results, "server_stats": stats,
+        "serving": results, "server_stats": stats, "clocks": sampler.summary(),
     }
 
 
@@ -741,11 +804,20 @@ def run_batching(args):
             b["out"].sub_(st)
 
     res = {}
+    # The autotuner picks the batch schedule (CTAs per SM, sampler unit size,
+    # bucket size) on this batch, untimed; the timed runs use its choice.
+    default_tuning = C.get_batch_tuning()
+    best, best_ms, start_ms = C.batch_autotune(entries, stream=sh, repeats=2)
+    res["autotune"] = {"tuning": best.as_dict(), "tuned_ms": best_ms, "default_ms": start_ms,
+                       "default_tuning": default_tuning.as_dict()}
+    clocks = None
     for name, fn in (("one_batch_launch", batched), ("sequential_plain_calls", sequential)):
         for _ in range(args.warmup):
             fn()
         torch.cuda.synchronize()
         ts = []
+        sampler = ClockSampler(0)
+        sampler.__enter__()
         for _ in range(max(1, args.steps // 4)):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -754,6 +826,8 @@ def run_batching(args):
             e1.record(stream)
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
+        sampler.__exit__(None, None, None)
+        clocks = clocks or sampler.summary()
         ms = statistics.mean(ts)
         res[name] = {"ms": ms, "queries_per_s": total_q / (ms / 1e3), "problems_per_s": 256 / (ms / 1e3)}
     return {
@@ -764,7 +838,8 @@ def run_batching(args):
         "config": {"workload": "batching: 256 3D gravity problems, 1,024..1,048,576 sources "
                                "log-uniform, queries = sources (self term excluded), stochastic "
                                "BH budget 64-512, Octree2", "queries": total_q},
-        "batching": res,
+        "batching": res, "clocks": clocks,
+        "gpu_launches": 4 * max(1, args.steps // 4),
     }
 
 

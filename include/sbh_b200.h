@@ -180,6 +180,28 @@ typedef struct sbh_batch_item {
 } sbh_batch_item;
 int sbh_eval_batch(const sbh_batch_item* items, int n_items, void* stream);
 
+/* Schedule knobs of the batched pipeline.  Results never depend on them (the
+ * sampler's streams are keyed by query index, Barnes-Hut is exact per query);
+ * only the speed does. */
+typedef struct sbh_batch_tuning {
+  int32_t sampler_unit_queries; /* sampler queries per work unit, 1..64 (default 2) */
+  int32_t bucket_queries;       /* target queries per Morton bucket, 2..4096 (default 8) */
+  int32_t blocks_per_sm;        /* persistent CTAs per SM; 0 = as many as fit (default) */
+  int32_t reserved;
+} sbh_batch_tuning;
+void sbh_batch_tuning_init(sbh_batch_tuning* tuning);
+/* The tuning sbh_eval_batch uses on `device` (initially the defaults). */
+int sbh_batch_set_tuning(int device, const sbh_batch_tuning* tuning);
+int sbh_batch_get_tuning(int device, sbh_batch_tuning* tuning);
+/* Autotuner: evaluates the batch under candidate tunings -- coordinate descent
+ * over CTAs per SM, sampler unit size and bucket size, each candidate timed
+ * `repeats` times on `stream` after one untimed run -- installs the fastest as
+ * the device's tuning and returns it with its time and the starting tuning's
+ * time (ms, median of the repeats).  Blocks until done; the output buffers
+ * hold the batch's results afterwards. */
+int sbh_batch_autotune(const sbh_batch_item* items, int n_items, void* stream, int repeats,
+                       sbh_batch_tuning* best, float* best_ms, float* start_ms);
+
 /* ---- serving ---------------------------------------------------------------
  * No counterpart in the reference.  A server keeps trees resident on one
  * device and evaluates requests submitted from any thread with continuous
@@ -197,6 +219,8 @@ typedef struct sbh_server_config {
   int64_t slot_queries;            /* queries admitted per batch (default 1 << 20) */
   int32_t max_requests_per_batch;  /* default 4096 */
   int32_t reserved;
+  sbh_batch_tuning tuning;         /* schedule of every batch (defaults as
+                                      sbh_batch_tuning_init; e.g. from sbh_batch_autotune) */
 } sbh_server_config;
 
 typedef struct sbh_request_info {

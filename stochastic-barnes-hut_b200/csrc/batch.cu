@@ -140,8 +140,8 @@ __device__ __noinline__ void run_sbh(const DevTree& t, const BatchItem& it, long
                                      const int* ord, float* scratch, int* status) {
   const int lane = threadIdx.x & 31;
   const SbhWarpSmem<float> ws = sbh_carve<float>(scratch, t.root_children);
-  const long long s0 = u * kUnitQueriesSampler;
-  const long long s1 = min(it.nq, s0 + kUnitQueriesSampler);
+  const long long s0 = u * it.unit_queries;
+  const long long s1 = min(it.nq, s0 + it.unit_queries);
   for (long long s = s0; s < s1; s++) {
     const long long qi = ord ? (long long)__ldg(ord + s) : s;
     const float3 q = load_query<DIM>(it.q, it.nq, qi);
@@ -222,16 +222,18 @@ __global__ void __launch_bounds__(kEvalThreads, 8)
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Bucket capacity: at least 2 queries per bucket (the tuning's lower bound),
+// plus a bucket per request for requests below a full bucket.
 long long max_buckets(const BatchEngine::Limits& lim) {
-  return lim.max_queries / 8 + 2LL * lim.max_items + 1024;
+  return lim.max_queries / 2 + 2LL * lim.max_items + 1024;
 }
 
-int sort_bits_for(long long nq, int dim) {
-  // About 8 queries per bucket; 6 bits per axis (3D) / 9 (2D) at most.
+int sort_bits_for(long long nq, int dim, int bucket_queries) {
+  // About bucket_queries queries per bucket; 6 bits per axis (3D) / 9 (2D) at most.
   if (nq < 64) return 0;
   int bits = 0;
   const int cap = dim == 3 ? 6 : 9;
-  while (bits < cap && (1LL << (dim * (bits + 1))) * 8 <= nq) bits++;
+  while (bits < cap && (1LL << (dim * (bits + 1))) * bucket_queries <= nq) bits++;
   return bits;
 }
 
@@ -268,18 +270,23 @@ BatchEngine::BatchEngine(const Limits& lim, int sm_count) : lim_(lim), sm_count_
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_eval_kernel, kEvalThreads,
                                                 eval_smem_);
-  eval_blocks_ = std::max(1, per_sm) * sm_count_;
+  per_sm_ = std::max(1, per_sm);
 }
 
 BatchEngine::~BatchEngine() {
-  if (exec_) cudaGraphExecDestroy(exec_);
+  for (Graph& g : graphs_)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   if (h_stage_) cudaFreeHost(h_stage_);
   if (dev_) cudaFree(dev_);
 }
 
 std::string BatchEngine::plan(std::vector<BatchItem>& items,
-                              const std::vector<DevTree>& host_trees) const {
+                              const std::vector<DevTree>& host_trees,
+                              const Tuning& tuning) const {
   if (!dev_ || !h_stage_) return "batch engine has no device or pinned memory";
+  if (tuning.sampler_unit < 1 || tuning.sampler_unit > 64 || tuning.bucket_queries < 2 ||
+      tuning.bucket_queries > 4096 || tuning.blocks_per_sm < 0)
+    return "batch tuning out of range";
   if ((int)items.size() > lim_.max_items) return "too many requests in one batch";
   long long sort_base = 0, bucket_base = 0, unit_base = 0;
   for (BatchItem& it : items) {
@@ -288,14 +295,15 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
     if (t.depth + 2 > lim_.max_tree_depth + 2) return "tree deeper than the engine supports";
     if (t.root_children > lim_.max_root_children) return "tree root wider than the engine supports";
     const bool sorted = it.method == 1 || it.method == 3;  // vote keeps the caller's order
-    it.sort_bits = (sorted && it.sort_bits >= 0) ? sort_bits_for(it.nq, t.dim) : 0;
+    it.sort_bits =
+        (sorted && it.sort_bits >= 0) ? sort_bits_for(it.nq, t.dim, tuning.bucket_queries) : 0;
     it.dim = t.dim;
     it.sort_base = sort_base;
     it.bucket_base = bucket_base;
     it.buckets = it.sort_bits > 0 ? (1LL << (t.dim * it.sort_bits)) : 1;
     it.unit_base = unit_base;
-    const long long per_unit = it.method == 3 ? kUnitQueriesSampler : kUnitQueriesWarp;
-    it.units = (it.nq + per_unit - 1) / per_unit;
+    it.unit_queries = it.method == 3 ? tuning.sampler_unit : kUnitQueriesWarp;
+    it.units = (it.nq + it.unit_queries - 1) / it.unit_queries;
     sort_base += it.nq;
     bucket_base += it.buckets;
     unit_base += it.units;
@@ -305,11 +313,9 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
   return "";
 }
 
-cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status) {
-  if (exec_) {
-    cudaGraphExecDestroy(exec_);
-    exec_ = nullptr;
-  }
+cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status, int blocks,
+                                 cudaGraphExec_t* out) {
+  *out = nullptr;
   // Captured on a private stream (the caller's may be the legacy default
   // stream, which cannot be captured); the graph is launched on the caller's.
   cudaStream_t stream = nullptr;
@@ -331,28 +337,36 @@ cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status) {
   batch_scan_kernel<<<1, kScanThreads, 0, stream>>>(d_header_, d_hist_);
   batch_scatter_kernel<<<aux_blocks, kAuxThreads, 0, stream>>>(d_header_, d_items_, d_keys_,
                                                               d_hist_, d_order_);
-  batch_eval_kernel<<<eval_blocks_, kEvalThreads, eval_smem_, stream>>>(
+  batch_eval_kernel<<<blocks, kEvalThreads, eval_smem_, stream>>>(
       d_header_, d_items_, d_trees, d_order_, d_status, warp_words, stack_cap);
   e = cudaStreamEndCapture(stream, &graph);
   cudaStreamDestroy(stream);
   if (e != cudaSuccess) return e;
-  e = cudaGraphInstantiate(&exec_, graph, 0);
+  e = cudaGraphInstantiate(out, graph, 0);
   cudaGraphDestroy(graph);
-  if (e != cudaSuccess) {
-    exec_ = nullptr;
-    return e;
-  }
-  captured_trees_ = d_trees;
-  captured_status_ = d_status;
-  return cudaSuccess;
+  if (e != cudaSuccess) *out = nullptr;
+  return e;
 }
 
 cudaError_t BatchEngine::launch(const std::vector<BatchItem>& items, const DevTree* d_trees,
-                                int* d_status, cudaStream_t stream) {
+                                int* d_status, cudaStream_t stream, const Tuning& tuning) {
   if (!dev_ || !h_stage_) return cudaErrorMemoryAllocation;
-  if (!exec_ || captured_trees_ != d_trees || captured_status_ != d_status) {
-    cudaError_t e = capture(d_trees, d_status);
+  if (captured_trees_ != d_trees || captured_status_ != d_status) {
+    for (Graph& g : graphs_)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    graphs_.clear();
+    captured_trees_ = d_trees;
+    captured_status_ = d_status;
+  }
+  const int per_sm = tuning.blocks_per_sm > 0 ? std::min(tuning.blocks_per_sm, per_sm_) : per_sm_;
+  const int blocks = per_sm * sm_count_;
+  cudaGraphExec_t exec = nullptr;
+  for (const Graph& g : graphs_)
+    if (g.blocks == blocks) exec = g.exec;
+  if (!exec) {
+    cudaError_t e = capture(d_trees, d_status, blocks, &exec);
     if (e != cudaSuccess) return e;
+    graphs_.push_back(Graph{blocks, exec});
   }
   BatchHeader h = {};
   h.n_items = (int)items.size();
@@ -369,7 +383,7 @@ cudaError_t BatchEngine::launch(const std::vector<BatchItem>& items, const DevTr
   cudaError_t e = cudaMemcpyAsync(d_header_, st, o_items + sizeof(BatchItem) * items.size(),
                                   cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return e;
-  return cudaGraphLaunch(exec_, stream);
+  return cudaGraphLaunch(exec, stream);
 }
 
 }  // namespace sbh

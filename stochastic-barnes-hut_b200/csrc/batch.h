@@ -21,6 +21,7 @@ struct BatchItem {
   int samples;               // stochastic method
   float beta;                // Barnes-Hut
   int sort_bits;             // Morton bits per axis of the query bucketing (0: keep order)
+  int unit_queries;          // queries per work unit
   KParams kp;
   unsigned long long seed;   // stochastic method
   const float* q;            // device SoA [dim][nq]
@@ -47,13 +48,19 @@ struct BatchHeader {
   unsigned long long next_unit;  // work counter of the persistent kernel
 };
 
-// Queries per work unit (one warp task): Barnes-Hut and brute force evaluate
-// 32 queries per task (a lane each); the sampler gives each query a warp.
+// Queries per work unit (one warp task) of Barnes-Hut and brute force: 32,
+// a lane each.  The sampler gives each query a warp; its unit size is tuned.
 constexpr int kUnitQueriesWarp = 32;
-constexpr int kUnitQueriesSampler = 2;
 
 class BatchEngine {
  public:
+  // Schedule knobs (the autotuner's search space); results never depend on them.
+  struct Tuning {
+    int sampler_unit = 2;     // sampler queries per work unit
+    int bucket_queries = 8;   // target queries per Morton bucket
+    int blocks_per_sm = 0;    // persistent CTAs per SM (0: as many as fit)
+  };
+
   struct Limits {
     int max_items = 4096;
     long long max_queries = 1 << 20;   // sorted positions (sum of request sizes)
@@ -70,21 +77,29 @@ class BatchEngine {
 
   // Fills item bookkeeping (sort/bucket/unit ranges, sort bits) for `items`
   // in place and checks limits.  Returns an error string or "".
-  std::string plan(std::vector<BatchItem>& items, const std::vector<DevTree>& host_trees) const;
-  // Enqueues the batch on `stream` (items already planned): copies the item
-  // table and header from pinned staging, then launches the captured graph.
+  std::string plan(std::vector<BatchItem>& items, const std::vector<DevTree>& host_trees,
+                   const Tuning& tuning) const;
+  // Enqueues the batch on `stream` (items already planned with `tuning`):
+  // copies the item table and header from pinned staging, then launches the
+  // graph captured for the tuning's grid.
   cudaError_t launch(const std::vector<BatchItem>& items, const DevTree* d_trees,
-                     int* d_status, cudaStream_t stream);
+                     int* d_status, cudaStream_t stream, const Tuning& tuning);
 
   const Limits& limits() const { return lim_; }
   size_t device_bytes() const { return dev_bytes_; }
+  // CTAs per SM of the evaluation kernel at full occupancy.
+  int max_blocks_per_sm() const { return per_sm_; }
 
  private:
-  cudaError_t capture(const DevTree* d_trees, int* d_status);
+  struct Graph {
+    int blocks = 0;
+    cudaGraphExec_t exec = nullptr;
+  };
+  cudaError_t capture(const DevTree* d_trees, int* d_status, int blocks, cudaGraphExec_t* out);
 
   Limits lim_;
   int sm_count_;
-  int eval_blocks_ = 0;
+  int per_sm_ = 1;
   size_t eval_smem_ = 0;
   // device buffers
   void* dev_ = nullptr;
@@ -96,8 +111,8 @@ class BatchEngine {
   int* d_order_ = nullptr;
   // pinned staging of header + items
   void* h_stage_ = nullptr;
-  // captured pipeline
-  cudaGraphExec_t exec_ = nullptr;
+  // captured pipelines, one per evaluation grid size
+  std::vector<Graph> graphs_;
   const DevTree* captured_trees_ = nullptr;
   int* captured_status_ = nullptr;
 };

@@ -87,6 +87,7 @@ bool covers(const BatchEngine::Limits& have, const BatchEngine::Limits& need) {
 struct BatchContext {
   std::mutex mu;
   std::unique_ptr<BatchEngine> engine;
+  BatchEngine::Tuning tuning;
   DevTree* d_trees = nullptr;
   DevTree* h_trees = nullptr;  // pinned
   int tree_cap = 0;
@@ -100,45 +101,81 @@ BatchContext& batch_context(int device) {
   return ctx[device];
 }
 
-}  // namespace
+BatchEngine::Tuning to_engine(const sbh_batch_tuning& t) {
+  BatchEngine::Tuning e;
+  e.sampler_unit = t.sampler_unit_queries;
+  e.bucket_queries = t.bucket_queries;
+  e.blocks_per_sm = t.blocks_per_sm;
+  return e;
+}
 
-SBH_API int sbh_eval_batch(const sbh_batch_item* items, int n_items, void* stream_ptr) {
+sbh_batch_tuning from_engine(const BatchEngine::Tuning& e) {
+  sbh_batch_tuning t = {};
+  t.sampler_unit_queries = e.sampler_unit;
+  t.bucket_queries = e.bucket_queries;
+  t.blocks_per_sm = e.blocks_per_sm;
+  return t;
+}
+
+int check_tuning(const sbh_batch_tuning* t) {
+  if (!t) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null tuning");
+  if (t->sampler_unit_queries < 1 || t->sampler_unit_queries > 64)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "sampler_unit_queries must be in [1, 64]");
+  if (t->bucket_queries < 2 || t->bucket_queries > 4096)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "bucket_queries must be in [2, 4096]");
+  if (t->blocks_per_sm < 0 || t->blocks_per_sm > 64)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "blocks_per_sm must be in [0, 64]");
+  return SBH_OK;
+}
+
+// Checks a batch's items; returns the device, the distinct trees and the query total.
+int check_batch(const sbh_batch_item* items, int n_items, int* device,
+                std::vector<const sbh_gpu_tree*>* uniq, long long* total) {
   if (n_items < 0 || (n_items > 0 && !items))
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null item list");
-  if (n_items == 0) return sbh::ok();
-  const int device = items[0].tree ? items[0].tree->device : -1;
-  if (device < 0 || device >= 64) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null tree");
-  std::vector<const sbh_gpu_tree*> uniq;
-  long long total = 0;
+  *device = -1;
+  *total = 0;
+  if (n_items == 0) return SBH_OK;
+  *device = items[0].tree ? items[0].tree->device : -1;
+  if (*device < 0 || *device >= 64) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null tree");
   for (int i = 0; i < n_items; i++) {
     const sbh_batch_item& b = items[i];
     int st = sbh::check_eval_params(b.tree, &b.params, b.nq);
     if (st != SBH_OK) return st;
-    if (b.tree->device != device)
+    if (b.tree->device != *device)
       return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "all trees of a batch must be on one device");
     if (b.nq > 0 && (!b.d_queries || !b.d_results))
       return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
-    if (std::find(uniq.begin(), uniq.end(), b.tree) == uniq.end()) uniq.push_back(b.tree);
-    total += b.nq;
+    if (std::find(uniq->begin(), uniq->end(), b.tree) == uniq->end()) uniq->push_back(b.tree);
+    *total += b.nq;
   }
-  BatchContext& ctx = batch_context(device);
-  std::lock_guard<std::mutex> lock(ctx.mu);
-  sbh::DeviceGuard guard(device);
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-  if (ctx.pending) {
-    cudaError_t e = cudaEventSynchronize(ctx.done);
-    ctx.pending = false;
-    if (e != cudaSuccess) return sbh::cuda_fail(e, "previous batch");
-    int status = 0;
-    if (ctx.d_status) {
-      cudaMemcpy(&status, ctx.d_status, sizeof(int), cudaMemcpyDeviceToHost);
-      if (status) cudaMemset(ctx.d_status, 0, sizeof(int));
-    }
-    if (status)
-      return sbh::fail(SBH_ERR_DEVICE_LIMIT, "the previous batch on this device hit a "
-                                              "device-side bound (status bits " +
-                                                  std::to_string(status) + ")");
+  return SBH_OK;
+}
+
+// Waits for the context's previous batch and reports its device status.
+int retire_previous(BatchContext& ctx) {
+  if (!ctx.pending) return SBH_OK;
+  cudaError_t e = cudaEventSynchronize(ctx.done);
+  ctx.pending = false;
+  if (e != cudaSuccess) return sbh::cuda_fail(e, "previous batch");
+  int status = 0;
+  if (ctx.d_status) {
+    cudaMemcpy(&status, ctx.d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (status) cudaMemset(ctx.d_status, 0, sizeof(int));
   }
+  if (status)
+    return sbh::fail(SBH_ERR_DEVICE_LIMIT, "the previous batch on this device hit a "
+                                            "device-side bound (status bits " +
+                                                std::to_string(status) + ")");
+  return SBH_OK;
+}
+
+// Enqueues a checked batch on `stream` with `tuning` (context lock held, device current).
+int enqueue_batch(BatchContext& ctx, const sbh_batch_item* items, int n_items,
+                  const std::vector<const sbh_gpu_tree*>& uniq, long long total,
+                  cudaStream_t stream, const BatchEngine::Tuning& tuning) {
+  int st = retire_previous(ctx);
+  if (st != SBH_OK) return st;
   // Tree table.
   std::vector<DevTree> table;
   for (const sbh_gpu_tree* t : uniq) table.push_back(t->dev);
@@ -195,16 +232,146 @@ SBH_API int sbh_eval_batch(const sbh_batch_item* items, int n_items, void* strea
     it.nq = b.nq;
     plan.push_back(it);
   }
-  if (plan.empty()) return sbh::ok();
-  std::string err = ctx.engine->plan(plan, table);
+  if (plan.empty()) return SBH_OK;
+  std::string err = ctx.engine->plan(plan, table, tuning);
   if (!err.empty()) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, err);
   std::memcpy(ctx.h_trees, table.data(), sizeof(DevTree) * table.size());
   cudaError_t e = cudaMemcpyAsync(ctx.d_trees, ctx.h_trees, sizeof(DevTree) * table.size(),
                                   cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess) e = ctx.engine->launch(plan, ctx.d_trees, ctx.d_status, stream);
+  if (e == cudaSuccess) e = ctx.engine->launch(plan, ctx.d_trees, ctx.d_status, stream, tuning);
   if (e == cudaSuccess) e = cudaEventRecord(ctx.done, stream);
   if (e != cudaSuccess) return sbh::cuda_fail(e, "batch launch");
   ctx.pending = true;
+  return SBH_OK;
+}
+
+}  // namespace
+
+SBH_API int sbh_eval_batch(const sbh_batch_item* items, int n_items, void* stream_ptr) {
+  int device = -1;
+  long long total = 0;
+  std::vector<const sbh_gpu_tree*> uniq;
+  int st = check_batch(items, n_items, &device, &uniq, &total);
+  if (st != SBH_OK) return st;
+  if (n_items == 0) return sbh::ok();
+  BatchContext& ctx = batch_context(device);
+  std::lock_guard<std::mutex> lock(ctx.mu);
+  sbh::DeviceGuard guard(device);
+  st = enqueue_batch(ctx, items, n_items, uniq, total, static_cast<cudaStream_t>(stream_ptr),
+                     ctx.tuning);
+  return st == SBH_OK ? sbh::ok() : st;
+}
+
+SBH_API void sbh_batch_tuning_init(sbh_batch_tuning* tuning) {
+  if (tuning) *tuning = from_engine(BatchEngine::Tuning());
+}
+
+SBH_API int sbh_batch_set_tuning(int device, const sbh_batch_tuning* tuning) {
+  if (device < 0 || device >= 64) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "bad device index");
+  int st = check_tuning(tuning);
+  if (st != SBH_OK) return st;
+  BatchContext& ctx = batch_context(device);
+  std::lock_guard<std::mutex> lock(ctx.mu);
+  ctx.tuning = to_engine(*tuning);
+  return sbh::ok();
+}
+
+SBH_API int sbh_batch_get_tuning(int device, sbh_batch_tuning* tuning) {
+  if (device < 0 || device >= 64 || !tuning)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "bad device index or null tuning");
+  BatchContext& ctx = batch_context(device);
+  std::lock_guard<std::mutex> lock(ctx.mu);
+  *tuning = from_engine(ctx.tuning);
+  return sbh::ok();
+}
+
+SBH_API int sbh_batch_autotune(const sbh_batch_item* items, int n_items, void* stream_ptr,
+                               int repeats, sbh_batch_tuning* best, float* best_ms,
+                               float* start_ms) {
+  if (repeats < 1 || repeats > 100)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "repeats must be in [1, 100]");
+  int device = -1;
+  long long total = 0;
+  std::vector<const sbh_gpu_tree*> uniq;
+  int st = check_batch(items, n_items, &device, &uniq, &total);
+  if (st != SBH_OK) return st;
+  if (n_items == 0 || total == 0) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "empty batch");
+  BatchContext& ctx = batch_context(device);
+  std::lock_guard<std::mutex> lock(ctx.mu);
+  sbh::DeviceGuard guard(device);
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return sbh::fail(SBH_ERR_CUDA, "cudaEventCreate");
+  }
+  // Median device time of `repeats` runs after one untimed run.
+  auto time_of = [&](const BatchEngine::Tuning& t, float* ms) -> int {
+    int s = enqueue_batch(ctx, items, n_items, uniq, total, stream, t);
+    if (s != SBH_OK) return s;
+    std::vector<float> v;
+    for (int r = 0; r < repeats; r++) {
+      s = retire_previous(ctx);
+      if (s != SBH_OK) return s;
+      cudaEventRecord(e0, stream);
+      s = enqueue_batch(ctx, items, n_items, uniq, total, stream, t);
+      if (s != SBH_OK) return s;
+      cudaEventRecord(e1, stream);
+      cudaError_t e = cudaEventSynchronize(e1);
+      float x = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&x, e0, e1);
+      if (e != cudaSuccess) return sbh::cuda_fail(e, "autotune timing");
+      v.push_back(x);
+    }
+    s = retire_previous(ctx);
+    if (s != SBH_OK) return s;
+    std::sort(v.begin(), v.end());
+    *ms = v[v.size() / 2];
+    return SBH_OK;
+  };
+  BatchEngine::Tuning cur = ctx.tuning;
+  float cur_ms = 0.f;
+  st = time_of(cur, &cur_ms);
+  const float first_ms = cur_ms;
+  // Coordinate descent; a candidate must win by 2% to replace the incumbent.
+  const int max_bps = ctx.engine ? ctx.engine->max_blocks_per_sm() : 1;
+  for (int coord = 0; coord < 3 && st == SBH_OK; coord++) {
+    std::vector<int> values;
+    if (coord == 0) {
+      for (int v : {0, max_bps * 3 / 4, max_bps / 2, max_bps / 4})
+        if ((v == 0 || (v >= 1 && v < max_bps)) &&
+            std::find(values.begin(), values.end(), v) == values.end())
+          values.push_back(v);
+    } else if (coord == 1) {
+      values = {1, 2, 4, 8};
+    } else {
+      values = {4, 8, 16, 32};
+    }
+    BatchEngine::Tuning best_t = cur;
+    float best_t_ms = cur_ms;
+    for (int v : values) {
+      BatchEngine::Tuning t = cur;
+      int& field = coord == 0 ? t.blocks_per_sm : coord == 1 ? t.sampler_unit : t.bucket_queries;
+      if (field == v) continue;
+      field = v;
+      float ms = 0.f;
+      st = time_of(t, &ms);
+      if (st != SBH_OK) break;
+      if (ms < best_t_ms * 0.98f) {
+        best_t = t;
+        best_t_ms = ms;
+      }
+    }
+    cur = best_t;
+    cur_ms = best_t_ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != SBH_OK) return st;
+  ctx.tuning = cur;
+  if (best) *best = from_engine(cur);
+  if (best_ms) *best_ms = cur_ms;
+  if (start_ms) *start_ms = first_ms;
   return sbh::ok();
 }
 
@@ -315,11 +482,12 @@ int sbh_server::launch(int si) {
     items.push_back(it);
     total = a.slot_offset + a.count;
   }
-  std::string err = s.engine->plan(items, h_trees);
+  const BatchEngine::Tuning tuning = to_engine(cfg.tuning);
+  std::string err = s.engine->plan(items, h_trees, tuning);
   if (!err.empty()) return SBH_ERR_INVALID_ARGUMENT;
   cudaError_t e = cudaMemcpyAsync(s.d_q, s.h_q, sizeof(float) * 3 * total, cudaMemcpyHostToDevice,
                                   s.stream);
-  if (e == cudaSuccess) e = s.engine->launch(items, d_trees, s.d_status, s.stream);
+  if (e == cudaSuccess) e = s.engine->launch(items, d_trees, s.d_status, s.stream, tuning);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s.h_out, s.d_out, sizeof(float) * total, cudaMemcpyDeviceToHost, s.stream);
   if (e == cudaSuccess && s.want_counts)
@@ -430,6 +598,7 @@ SBH_API void sbh_server_config_init(sbh_server_config* cfg) {
   cfg->slots = 3;
   cfg->slot_queries = 1 << 20;
   cfg->max_requests_per_batch = 4096;
+  sbh_batch_tuning_init(&cfg->tuning);
 }
 
 SBH_API int sbh_server_create(const sbh_server_config* cfg_in, sbh_server** out) {
@@ -443,6 +612,7 @@ SBH_API int sbh_server_create(const sbh_server_config* cfg_in, sbh_server** out)
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "slot_queries must be in [1, 2^28]");
   if (cfg.max_requests_per_batch < 1 || cfg.max_requests_per_batch > (1 << 20))
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "max_requests_per_batch must be in [1, 2^20]");
+  if (check_tuning(&cfg.tuning) != SBH_OK) return SBH_ERR_INVALID_ARGUMENT;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg.device < 0 || cfg.device >= ndev) {
     cudaGetLastError();

@@ -64,6 +64,10 @@ _SIGNATURES = {
     "sbh_eval_grad": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _P]),
     "sbh_eval_grad_device": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P]),
     "sbh_measure_pipe_rates": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P]),
+    "sbh_batch_tuning_init": (None, [_P]),
+    "sbh_batch_set_tuning": (ctypes.c_int, [ctypes.c_int, _P]),
+    "sbh_batch_get_tuning": (ctypes.c_int, [ctypes.c_int, _P]),
+    "sbh_batch_autotune": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int, _P, _P, _P]),
 }
 
 # Largest query count sbh_eval_device_static_scratch accepts per call.
@@ -91,10 +95,19 @@ class BatchItem(ctypes.Structure):
                 ("d_results", _P), ("d_contribs", _P), ("d_self_mass", _P)]
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("sampler_unit_queries", ctypes.c_int32), ("bucket_queries", ctypes.c_int32),
+                ("blocks_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {"sampler_unit_queries": self.sampler_unit_queries,
+                "bucket_queries": self.bucket_queries, "blocks_per_sm": self.blocks_per_sm}
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("slots", ctypes.c_int32),
                 ("slot_queries", ctypes.c_int64), ("max_requests_per_batch", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("reserved", ctypes.c_int32), ("tuning", BatchTuning)]
 
 
 class RequestInfo(ctypes.Structure):
@@ -299,9 +312,7 @@ class GpuTree:
         self.close()
 
 
-def eval_batch(entries, stream: int = 0):
-    """sbh_eval_batch: entries are (gpu_tree, params, d_queries, nq, d_results,
-    d_contribs or 0, d_self_mass or 0) with device pointers; one pipeline for all."""
+def _batch_items(entries):
     arr = (BatchItem * len(entries))()
     for i, (tree, p, dq, nq, dout, dcnt, dself) in enumerate(entries):
         arr[i].tree = tree.handle
@@ -311,7 +322,47 @@ def eval_batch(entries, stream: int = 0):
         arr[i].d_results = dout
         arr[i].d_contribs = dcnt or None
         arr[i].d_self_mass = dself or None
-    _check(lib().sbh_eval_batch(arr, len(entries), ctypes.c_void_p(stream)))
+    return arr
+
+
+def eval_batch(entries, stream: int = 0):
+    """sbh_eval_batch: entries are (gpu_tree, params, d_queries, nq, d_results,
+    d_contribs or 0, d_self_mass or 0) with device pointers; one pipeline for all."""
+    _check(lib().sbh_eval_batch(_batch_items(entries), len(entries), ctypes.c_void_p(stream)))
+
+
+def batch_tuning(sampler_unit_queries=None, bucket_queries=None, blocks_per_sm=None) -> BatchTuning:
+    """A tuning with the library defaults, overridden where given."""
+    t = BatchTuning()
+    lib().sbh_batch_tuning_init(ctypes.byref(t))
+    if sampler_unit_queries is not None:
+        t.sampler_unit_queries = sampler_unit_queries
+    if bucket_queries is not None:
+        t.bucket_queries = bucket_queries
+    if blocks_per_sm is not None:
+        t.blocks_per_sm = blocks_per_sm
+    return t
+
+
+def set_batch_tuning(t: BatchTuning, device: int = 0):
+    _check(lib().sbh_batch_set_tuning(device, ctypes.byref(t)))
+
+
+def get_batch_tuning(device: int = 0) -> BatchTuning:
+    t = BatchTuning()
+    _check(lib().sbh_batch_get_tuning(device, ctypes.byref(t)))
+    return t
+
+
+def batch_autotune(entries, stream: int = 0, repeats: int = 3):
+    """sbh_batch_autotune: returns (best tuning, best ms, starting tuning's ms);
+    the best is installed for later sbh_eval_batch calls on the device."""
+    best = BatchTuning()
+    best_ms, start_ms = ctypes.c_float(0), ctypes.c_float(0)
+    _check(lib().sbh_batch_autotune(_batch_items(entries), len(entries), ctypes.c_void_p(stream),
+                                    repeats, ctypes.byref(best), ctypes.byref(best_ms),
+                                    ctypes.byref(start_ms)))
+    return best, best_ms.value, start_ms.value
 
 
 def measure_pipe_rates(device: int = 0) -> dict:
@@ -348,11 +399,14 @@ class Request:
 class Server:
     """sbh_server_*: resident trees and continuous batching on one device."""
 
-    def __init__(self, device=0, slots=3, slot_queries=1 << 20, max_requests_per_batch=4096):
+    def __init__(self, device=0, slots=3, slot_queries=1 << 20, max_requests_per_batch=4096,
+                 tuning: BatchTuning | None = None):
         cfg = ServerConfig()
         lib().sbh_server_config_init(ctypes.byref(cfg))
         cfg.device, cfg.slots, cfg.slot_queries = device, slots, slot_queries
         cfg.max_requests_per_batch = max_requests_per_batch
+        if tuning is not None:
+            cfg.tuning = tuning
         h = ctypes.c_void_p()
         _check(lib().sbh_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self.handle = h

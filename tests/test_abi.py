@@ -30,12 +30,42 @@ def test_ctypes_binding_covers_the_header():
     assert sorted(C._SIGNATURES) == declared_functions()
 
 
-def test_struct_layouts():
-    assert ctypes.sizeof(C.Params) == 40
-    assert ctypes.sizeof(C.TreeInfo) == 56
-    assert ctypes.sizeof(C.BatchItem) == 88
-    assert ctypes.sizeof(C.ServerConfig) == 24
-    assert ctypes.sizeof(C.RequestInfo) == 32
+STRUCTS = {  # C name -> ctypes mirror
+    "sbh_params": C.Params, "sbh_tree_info": C.TreeInfo, "sbh_batch_item": C.BatchItem,
+    "sbh_batch_tuning": C.BatchTuning, "sbh_server_config": C.ServerConfig,
+    "sbh_request_info": C.RequestInfo, "sbh_server_stats": C.ServerStats,
+}
+
+
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """Size and every field offset of each ABI struct, as gcc lays it out from
+    the header, equal the ctypes mirror's."""
+    import shutil
+    import subprocess
+
+    import pytest
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", f'#include "{HEADER}"',
+             "int main(void) {"]
+    for cname, cls in STRUCTS.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-o", str(exe), str(src)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                               text=True).stdout.splitlines():
+        cname, what, v = line.split()
+        got[(cname, what)] = int(v)
+    for cname, cls in STRUCTS.items():
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)
     assert C.lib().sbh_abi_version() == 1
 
 

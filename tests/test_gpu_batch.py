@@ -159,3 +159,82 @@ def test_server_rejects_bad_requests(env):
     r = server.submit(tid, np.zeros((0, 3), np.float32), C.params(method=C.BARNES_HUT))
     assert r.wait().shape == (0,)
     server.close()
+
+
+def _batch(env, rng_seed=96):
+    torch, trees, gpus = env
+    rng = np.random.default_rng(rng_seed)
+    entries, keep = [], []
+    for name, method, kernel, nq, extra in REQUESTS:
+        dim = gpus[name].dim
+        q = rng.uniform(-1.2, 1.2, (nq, dim)).astype(np.float32)
+        p = C.params(method=method, kernel=kernel, **extra)
+        dq = _dev(torch, q) if nq else torch.empty((dim, 1), device="cuda")
+        out = torch.zeros(max(nq, 1), dtype=torch.float32, device="cuda")
+        entries.append((gpus[name], p, dq.data_ptr(), nq, out.data_ptr(), 0, 0))
+        keep.append((dq, out, nq))
+    return entries, keep
+
+
+def test_batch_results_do_not_depend_on_tuning(env):
+    torch = env[0]
+    entries, keep = _batch(env)
+    stream = torch.cuda.current_stream().cuda_stream
+    default = C.get_batch_tuning()
+    outs = []
+    try:
+        for t in (C.batch_tuning(), C.batch_tuning(sampler_unit_queries=1, bucket_queries=32),
+                  C.batch_tuning(sampler_unit_queries=8, bucket_queries=2, blocks_per_sm=1)):
+            C.set_batch_tuning(t)
+            for _, out, _ in keep:
+                out.zero_()
+            C.eval_batch(entries, stream=stream)
+            torch.cuda.synchronize()
+            outs.append([out.cpu().numpy()[:nq].copy() for _, out, nq in keep])
+    finally:
+        C.set_batch_tuning(default)
+    for other in outs[1:]:
+        for a, b in zip(outs[0], other):
+            assert bits_equal(a, b)
+    with pytest.raises(C.SbhError):
+        C.set_batch_tuning(C.batch_tuning(sampler_unit_queries=0))
+    with pytest.raises(C.SbhError):
+        C.set_batch_tuning(C.batch_tuning(bucket_queries=1))
+
+
+def test_autotune_installs_a_valid_tuning(env):
+    torch, trees, gpus = env
+    entries, keep = _batch(env, rng_seed=97)
+    stream = torch.cuda.current_stream().cuda_stream
+    default = C.get_batch_tuning()
+    try:
+        best, best_ms, start_ms = C.batch_autotune(entries, stream=stream, repeats=2)
+        assert 0 < best_ms <= start_ms
+        assert 1 <= best.sampler_unit_queries <= 64 and 2 <= best.bucket_queries <= 4096
+        assert best.blocks_per_sm >= 0
+        assert C.get_batch_tuning().as_dict() == best.as_dict()
+        # the buffers hold the batch's results
+        torch.cuda.synchronize()
+        for (name, method, kernel, nq, extra), (dq, out, _) in zip(REQUESTS, keep):
+            if nq == 0:
+                continue
+            q = dq.cpu().numpy().T.copy()
+            want, _ = gpus[name].eval(q, C.params(method=method, kernel=kernel, **extra))
+            _check_same(method, kernel, out.cpu().numpy()[:nq], want)
+    finally:
+        C.set_batch_tuning(default)
+
+
+def test_server_with_a_tuning(env):
+    torch, trees, gpus = env
+    t = C.batch_tuning(sampler_unit_queries=4, bucket_queries=16, blocks_per_sm=2)
+    server = C.Server(slots=2, slot_queries=8192, tuning=t)
+    tid = server.add_tree(trees["torus2"])
+    q = np.random.default_rng(98).uniform(-1.2, 1.2, (5000, 3)).astype(np.float32)
+    p = C.params(method=C.STOCHASTIC, kernel=C.WINDING_NUMBER, samples_per_subdomain=2, seed=3)
+    r = server.submit(tid, q, p)
+    want, _ = gpus["torus2"].eval(q, p)
+    assert bits_equal(r.wait(), want)
+    server.close()
+    with pytest.raises(C.SbhError):
+        C.Server(slots=1, slot_queries=1024, tuning=C.batch_tuning(bucket_queries=0))
