@@ -151,9 +151,12 @@ int sbh_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* queries,
 /* ---- evaluation, device buffers (asynchronous) -------------------------------
  * Same computation with d_queries/d_results (and optional d_contribs) in device
  * memory of the tree's device; enqueued on `stream`, returns without waiting.
- * Temporary device memory comes from the stream-ordered allocator of that
- * stream.  Device-side limit violations are reported by the next blocking call
- * on the same tree, or by sbh_gpu_tree_check. */
+ * Temporary device memory (the query order of Barnes-Hut and the sampler, about
+ * 8 bytes per query) is allocated stream-ordered on `stream` from a memory pool
+ * the library keeps per device; the pool holds on to freed memory, so it keeps
+ * the largest call's scratch reserved until the process exits.  Device-side
+ * limit violations are reported by the next blocking call on the same tree, or
+ * by sbh_gpu_tree_check. */
 int sbh_eval_device(sbh_gpu_tree* tree, const sbh_params* params, const float* d_queries,
                     int64_t nq, float* d_results, int32_t* d_contribs, void* stream);
 

@@ -21,28 +21,45 @@ namespace {
 constexpr int BH_THREADS = 128;
 constexpr int BH_WARPS = BH_THREADS / 32;
 
+// Each warp takes `group` consecutive (sorted) queries, one per lane.
 template <int DIM, int K, bool VOTE>
 __global__ void __launch_bounds__(BH_THREADS)
     barnes_hut_kernel(DevTree t, const float* __restrict__ qsoa, long long nq,
                       const int* __restrict__ order, float beta, KParams kp,
                       float* __restrict__ out, int* __restrict__ contribs, int* status,
-                      int stack_cap) {
+                      int stack_cap, int group) {
   extern __shared__ BhStackEntry s_stack[];
   const int warp = threadIdx.x >> 5;
-  const long long slot0 = ((long long)blockIdx.x * BH_WARPS + warp) * 32;
-  bh_warp_task<DIM, K, VOTE>(t, qsoa, nq, order, slot0, min(slot0 + 32, nq), beta, kp, out,
+  const long long slot0 = ((long long)blockIdx.x * BH_WARPS + warp) * group;
+  bh_warp_task<DIM, K, VOTE>(t, qsoa, nq, order, slot0, min(slot0 + group, nq), beta, kp, out,
                              contribs, status, s_stack + warp * stack_cap, stack_cap, nullptr);
+}
+
+// Queries per warp.  A warp's walk covers the union of its lanes' opened sets
+// and each step waits on a node load, so the kernel is latency-bound; when the
+// query count cannot give every SM about 48 warps of 32 queries, warps take
+// fewer queries (down to 4) to have more walks in flight.  Per-query results
+// do not depend on the grouping.  Vote mode keeps 32: its acceptance is defined
+// over 32 consecutive queries.
+int queries_per_warp(long long nq, bool vote, int sm_count) {
+  if (vote) return 32;
+  const long long want = 48LL * sm_count;
+  int g = 32;
+  while (g > 4 && (nq + g - 1) / g < want) g /= 2;
+  return g;
 }
 
 template <int DIM, int K, bool VOTE>
 cudaError_t launch_bh(const DevTree& t, const float* q, long long nq, const int* order, float beta,
                       const KParams& kp, float* out, int* contribs, int* status,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, int sm_count) {
   const int stack_cap = t.depth + 2;
   const size_t smem = (size_t)BH_WARPS * stack_cap * sizeof(BhStackEntry);
-  const long long blocks = (nq + BH_THREADS - 1) / BH_THREADS;
+  const int group = queries_per_warp(nq, VOTE, sm_count);
+  const long long warps = (nq + group - 1) / group;
+  const long long blocks = (warps + BH_WARPS - 1) / BH_WARPS;
   barnes_hut_kernel<DIM, K, VOTE><<<(unsigned)blocks, BH_THREADS, smem, stream>>>(
-      t, q, nq, order, beta, kp, out, contribs, status, stack_cap);
+      t, q, nq, order, beta, kp, out, contribs, status, stack_cap, group);
   return cudaGetLastError();
 }
 
@@ -50,14 +67,15 @@ cudaError_t launch_bh(const DevTree& t, const float* q, long long nq, const int*
 
 cudaError_t launch_barnes_hut(const DevTree& t, int kernel, bool vote, const float* q,
                               long long nq, const int* order, float beta, const KParams& kp,
-                              float* out, int* contribs, int* status, cudaStream_t stream) {
+                              float* out, int* contribs, int* status, cudaStream_t stream,
+                              int sm_count) {
   if (nq <= 0) return cudaSuccess;
 #define SBH_BH_CASE(D, K)                                                                   \
   if (t.dim == D && kernel == K)                                                            \
     return vote ? launch_bh<D, K, true>(t, q, nq, order, beta, kp, out, contribs, status,   \
-                                        stream)                                             \
+                                        stream, sm_count)                                   \
                 : launch_bh<D, K, false>(t, q, nq, order, beta, kp, out, contribs, status,  \
-                                         stream);
+                                         stream, sm_count);
   SBH_BH_CASE(3, kGravity)
   SBH_BH_CASE(3, kWindingNumber)
   SBH_BH_CASE(3, kSmoothDist)

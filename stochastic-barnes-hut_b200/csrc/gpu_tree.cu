@@ -61,13 +61,44 @@ cudaError_t run_eval(sbh_gpu_tree* tree, const sbh_params* p, const float* d_q, 
     case SBH_METHOD_BARNES_HUT_VOTE:
       return sbh::launch_barnes_hut(t, p->kernel, p->method == SBH_METHOD_BARNES_HUT_VOTE, d_q,
                                     nq, order, p->beta, kp, d_out, d_contribs, tree->d_status,
-                                    stream);
+                                    stream, tree->sm_count);
     case SBH_METHOD_STOCHASTIC:
       return sbh::launch_stochastic(t, p->kernel, d_q, nq, order, p->samples_per_subdomain,
                                     p->seed, kp, d_out, d_contribs, tree->d_status, stream,
                                     tree->sm_count);
   }
   return cudaErrorInvalidValue;
+}
+
+// Stream-ordered scratch of the asynchronous entry points comes from a pool of
+// the library's own per device, which keeps freed memory reserved (release
+// threshold: unlimited): a process's default pool hands memory back to the
+// driver at every synchronisation, so each call would map its scratch afresh.
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+
+int scratch_pool(int device, cudaMemPool_t* out) {
+  if (device < 0 || device >= 64) return sbh::fail(SBH_ERR_UNSUPPORTED, "device index beyond 64");
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pools[device]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return sbh::cuda_fail(e, "cudaMemPoolCreate(scratch)");
+    uint64_t keep = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+      cudaMemPoolDestroy(pool);
+      return sbh::cuda_fail(e, "cudaMemPoolSetAttribute(scratch)");
+    }
+    g_pools[device] = pool;
+  }
+  *out = g_pools[device];
+  return SBH_OK;
 }
 
 // Extra checks of the gradient entry points.
@@ -163,8 +194,12 @@ int device_eval(sbh_gpu_tree* tree, const sbh_params* params, const float* d_que
   void* d_sort = nullptr;
   if (wants_sort(params)) {
     const size_t b_ord = align256((size_t)nq * sizeof(int));
-    SBH_CK(cudaMallocAsync(&tmp, b_ord + sbh::query_sort_workspace_bytes(nq), stream),
-           "cudaMallocAsync(workspace)");
+    cudaMemPool_t pool = nullptr;
+    st = scratch_pool(tree->device, &pool);
+    if (st != SBH_OK) return st;
+    SBH_CK(cudaMallocFromPoolAsync(&tmp, b_ord + sbh::query_sort_workspace_bytes(nq), pool,
+                                   stream),
+           "cudaMallocFromPoolAsync(workspace)");
     d_ord = static_cast<int*>(tmp);
     d_sort = static_cast<char*>(tmp) + b_ord;
   }

@@ -12,7 +12,8 @@ cudaError_t launch_brute_force(const DevTree& t, int kernel, const float* q, lon
 
 cudaError_t launch_barnes_hut(const DevTree& t, int kernel, bool vote, const float* q,
                               long long nq, const int* order, float beta, const KParams& kp,
-                              float* out, int* contribs, int* status, cudaStream_t stream);
+                              float* out, int* contribs, int* status, cudaStream_t stream,
+                              int sm_count);
 
 cudaError_t launch_stochastic(const DevTree& t, int kernel, const float* q, long long nq,
                               const int* order, int samples, unsigned long long seed,

@@ -27,6 +27,36 @@
 
 namespace sbh {
 
+// Fast-path kernel values: same functions as kernel_exact, evaluated with FMA
+// and the hardware reciprocal square root (brute force only).
+template <int DIM, int K>
+__device__ __forceinline__ float kernel_fast(float4 s, float4 nr, float3 q, const KParams& kp) {
+  const float dx = s.x - q.x, dy = s.y - q.y, dz = DIM == 3 ? s.z - q.z : 0.f;
+  if (K == kPlummer) {
+    float r2 = fmaf(dx, dx, kp.eps2);
+    r2 = fmaf(dy, dy, r2);
+    if (DIM == 3) r2 = fmaf(dz, dz, r2);
+    return s.w * rsqrtf(r2);
+  }
+  float r2 = dx * dx;
+  r2 = fmaf(dy, dy, r2);
+  if (DIM == 3) r2 = fmaf(dz, dz, r2);
+  if (K == kGravity) {
+    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+    return __fdividef(-s.w, r + 1e-1f);
+  } else if (K == kWindingNumber) {
+    float qdn = nr.x * dx;
+    qdn = fmaf(nr.y, dy, qdn);
+    if (DIM == 3) qdn = fmaf(nr.z, dz, qdn);
+    if (DIM == 2) return __fdividef(s.w * qdn, kTwoPi * (r2 + 1e-5f));
+    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+    return __fdividef(s.w * qdn, kFourPi * fmaf(r2, r, 1e-5f));
+  } else {  // smooth distance
+    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+    return expf(-kp.alpha * r);
+  }
+}
+
 template <int DIM, int K>
 struct SumF {
   using V = float;
