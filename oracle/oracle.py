@@ -69,7 +69,7 @@ def oracle_lib() -> ctypes.CDLL:
         lib.orc_bh.argtypes = [_P, ctypes.c_int, _P, _I64, _F, _F, _P, _P, _P]
         lib.orc_bh_vote.argtypes = [_P, ctypes.c_int, _P, _I64, _F, _F, ctypes.c_int, _P, _P]
         lib.orc_sbh.argtypes = [_P, ctypes.c_int, _P, _I64, ctypes.c_int, ctypes.c_int,
-                                ctypes.c_uint64, _P, _F, _P, _P]
+                                ctypes.c_uint64, _P, _F, _P, _P, _P]
         lib.orc_brute_force_f64.argtypes = [_P, _P, _P, _I64, ctypes.c_int, ctypes.c_int, _F, _F,
                                             _P, _I64, _P]
         lib.orc_brute_force_abs_f64.argtypes = lib.orc_brute_force_f64.argtypes
@@ -211,15 +211,19 @@ class OracleTree(_TreeBase):
                              _ptr(out), _ptr(cnt))
         return out, cnt
 
-    def sbh(self, kernel, queries, samples, rng=RNG_PHILOX, seed=0, mt_seeds=None, eps=1e-3):
+    def sbh(self, kernel, queries, samples, rng=RNG_PHILOX, seed=0, mt_seeds=None, eps=1e-3,
+            return_scale=False):
+        """(values, counts[, scales]): scales are the per-query magnitudes of all
+        summed terms (see orc_sbh), for tolerances between summation orders."""
         q = _f32(queries, (-1, self.dim))
         nq = q.shape[0]
         out = np.zeros(nq, np.float32)
         cnt = np.zeros(nq, np.int32)
+        sc = np.zeros(nq, np.float64) if return_scale else None
         ms = None if mt_seeds is None else np.ascontiguousarray(mt_seeds, np.uint32)
         self.lib.orc_sbh(self._h, kernel, _ptr(q), nq, samples, rng, seed, _ptr(ms), eps,
-                         _ptr(out), _ptr(cnt))
-        return out, cnt
+                         _ptr(out), _ptr(cnt), _ptr(sc))
+        return (out, cnt, sc) if return_scale else (out, cnt)
 
 
     def bh_grad(self, kernel, queries, beta, alpha=1.0, eps=1e-3):

@@ -651,6 +651,7 @@ typedef struct {
   float* out;
   int32_t* counts;
   uint64_t* hashes;
+  double* scales;
 } eval_ctx;
 
 static void bh_body(void* vc, int64_t i) {
@@ -664,7 +665,7 @@ static void bh_body(void* vc, int64_t i) {
 
 void orc_bh(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta, float eps,
             float* out, int32_t* counts, uint64_t* hashes) {
-  eval_ctx c = {t, kernel, 0, 0, 0, q, nq, beta, eps, 0, NULL, out, counts, hashes};
+  eval_ctx c = {t, kernel, 0, 0, 0, q, nq, beta, eps, 0, NULL, out, counts, hashes, NULL};
   par_for(nq, 16, bh_body, &c);
 }
 
@@ -810,7 +811,7 @@ static void bh_vote_body(void* vc, int64_t g) {
 
 void orc_bh_vote(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta,
                  float eps, int group, float* out, int32_t* counts) {
-  eval_ctx c = {t, kernel, group, 0, 0, q, nq, beta, eps, 0, NULL, out, counts, NULL};
+  eval_ctx c = {t, kernel, group, 0, 0, q, nq, beta, eps, 0, NULL, out, counts, NULL, NULL};
   par_for((nq + group - 1) / group, 4, bh_vote_body, &c);
 }
 
@@ -926,11 +927,13 @@ static float rng_uniform(orc_rng* r) {
 
 /* multiLevelPrefixControlVariateSample_stackless, include/tree_sampler.h:21-113. */
 static float sbh_one(const orc_tree* t, int kernel, const float* q, int samples, orc_rng* rng,
-                     float eps, int32_t* total_contribs) {
+                     float eps, int32_t* total_contribs, double* scale_out) {
   float bh = 0, mlcv = 0;
   int tc = 0;
+  double scale = 0; /* magnitude of everything summed: sum of |term| x |weight| */
   if (t->leaf[0]) { /* a single-leaf tree has no root children to sample */
     *total_contribs = 0;
+    if (scale_out) *scale_out = 0;
     return 0;
   }
   const uint64_t* rm = t->mask;
@@ -940,11 +943,15 @@ static float sbh_one(const orc_tree* t, int kernel, const float* q, int samples,
     int64_t S = t->child[b];
     if (t->leaf[S]) {
       for (int64_t i = t->start[S]; i < t->end[S]; i++) {
-        bh += kern_point(t, kernel, i, q, eps);
+        float k = kern_point(t, kernel, i, q, eps);
+        bh += k;
+        scale += fabs((double)k);
         tc++;
       }
     } else {
-      bh += kern_node(t, kernel, S, q, eps);
+      float k = kern_node(t, kernel, S, q, eps);
+      bh += k;
+      scale += fabs((double)k);
       tc++;
     }
     uint64_t nS = (uint64_t)(t->end[S] - t->start[S]);
@@ -978,29 +985,37 @@ static float sbh_one(const orc_tree* t, int kernel, const float* q, int samples,
         cb = (cb < ffr) ? ffr : cb; /* std::max(cur_beta, far_field_ratio) */
         float prev_res = kern_node(t, kernel, prev, q, eps);
         float cur_res = 0;
+        double abs_res = fabs((double)prev_res);
         const uint64_t* pm = t->mask + prev * t->mw;
         for (uint64_t cbit = first_bit(pm, t->mw, t->bf); cbit < (uint64_t)t->bf;
              cbit = next_bit(pm, t->mw, t->bf, cbit)) {
           int64_t c = t->child[prev * t->bf + cbit];
           if (t->leaf[c]) {
             for (int64_t i = t->start[c]; i < t->end[c]; i++) {
-              cur_res += kern_point(t, kernel, i, q, eps);
+              float k = kern_point(t, kernel, i, q, eps);
+              cur_res += k;
+              abs_res += fabs((double)k);
               tc++;
             }
           } else {
-            cur_res += kern_node(t, kernel, c, q, eps);
+            float k = kern_node(t, kernel, c, q, eps);
+            cur_res += k;
+            abs_res += fabs((double)k);
             tc++;
           }
         }
         float diff = cur_res - prev_res;
-        float wd = spi / (ev * (float)(uint64_t)(t->end[prev] - t->start[prev])) * diff;
+        float w = spi / (ev * (float)(uint64_t)(t->end[prev] - t->start[prev]));
+        float wd = w * diff;
         wda += wd;
+        scale += fabs((double)w) * abs_res / samples;
       }
       sub_total += wda;
     }
     mlcv += sub_total / (float)samples;
   }
   *total_contribs = tc;
+  if (scale_out) *scale_out = scale;
   return bh + mlcv;
 }
 
@@ -1017,14 +1032,16 @@ static void sbh_body(void* vc, int64_t i) {
     r.query = (uint64_t)i;
   }
   int32_t n = 0;
-  c->out[i] = sbh_one(c->t, c->kernel, c->q + i * c->t->dim, c->samples, &r, c->eps, &n);
+  c->out[i] = sbh_one(c->t, c->kernel, c->q + i * c->t->dim, c->samples, &r, c->eps, &n,
+                      c->scales ? c->scales + i : NULL);
   if (c->counts) c->counts[i] = n;
 }
 
 void orc_sbh(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
              int rng_mode, uint64_t seed, const uint32_t* mt_seeds, float eps, float* out,
-             int32_t* counts) {
-  eval_ctx c = {t, kernel, 0, samples, rng_mode, q, nq, 0, eps, seed, mt_seeds, out, counts, NULL};
+             int32_t* counts, double* scales) {
+  eval_ctx c = {t, kernel, 0, samples, rng_mode, q, nq, 0, eps, seed, mt_seeds, out, counts, NULL,
+                scales};
   par_for(nq, 16, sbh_body, &c);
 }
 

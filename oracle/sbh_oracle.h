@@ -63,10 +63,13 @@ void orc_bh_vote(const orc_tree* t, int kernel, const float* q, int64_t nq, floa
                  float eps, int group, float* out, int32_t* counts);
 /* Stochastic Barnes-Hut (multi-level prefix control variate).
  * rng_mode ORC_RNG_MT19937 seeds std::mt19937 with mt_seeds[i] for query i;
- * ORC_RNG_PHILOX uses `seed` as the Philox key and the query index as counter. */
+ * ORC_RNG_PHILOX uses `seed` as the Philox key and the query index as counter.
+ * scales (optional): per query, the sum of the magnitudes of everything the
+ * estimate adds up (|BH term| + |path weight| x sum |k| of each expansion /
+ * samples) -- the scale of rounding differences between summation orders. */
 void orc_sbh(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
              int rng_mode, uint64_t seed, const uint32_t* mt_seeds, float eps, float* out,
-             int32_t* counts);
+             int32_t* counts, double* scales);
 /* FP64 brute force over raw points (row-major), alpha and eps given explicitly. */
 void orc_brute_force_f64(const float* pts, const float* nrm, const float* mass, int64_t n,
                          int dim, int kernel, float alpha, float eps, const float* q,

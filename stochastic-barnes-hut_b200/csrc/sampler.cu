@@ -17,9 +17,10 @@
 //   * Expansions.  Whenever some lanes each need the children sum of a node
 //     (its "expansion"), the warp lays the children of all those nodes out as
 //     one flat list and evaluates it 32 entries at a time -- consecutive
-//     children are consecutive node records, so the loads coalesce -- into
-//     shared memory.  Each owning lane then adds its own node's values in cell
-//     order, so the sum is the reference's sum bit for bit.
+//     children are consecutive node records, so the loads coalesce -- and a
+//     segmented scan across the lanes (one segment per node) forms every
+//     node's children sum at once, so no lane adds children one by one while
+//     the others wait.
 //   * Phase A, lanes over subdomains: the BH term of S and the first path step
 //     from S (taken by every sample of S: its continuation probability is 1),
 //     expanded once per subdomain instead of once per sample.
@@ -29,12 +30,14 @@
 //     own Philox4x32-10 stream keyed by (seed, query index, path index), so
 //     results do not depend on launch shape, batching or query order.
 //   * Lane 0 adds the per-path corrections and BH terms in the reference's order.
-// With identical random decisions every FP32 operation matches the reference
-// CPU estimator (IEEE single rounding throughout, see device_common.cuh); the
-// oracle drives its restatement with the same Philox stream and the tests
-// compare bit for bit.  The reference's GPU kernel (seed 0, streams shared
-// across queries, per-block sample indices, tree_sampler_gpu.h:41-42,69-71) is
-// replaced by independent per-query streams.
+// With identical random decisions the estimator takes exactly the reference
+// CPU estimator's paths and terms, each term rounded as the reference rounds it
+// (IEEE single rounding, see device_common.cuh); only each node's children sum
+// is added as a balanced tree instead of left to right.  The oracle drives its
+// restatement with the same Philox stream: contribution counts match exactly
+// and values to a few ulp of the summed magnitudes.  The reference's GPU
+// kernel (seed 0, streams shared across queries, per-block sample indices,
+// tree_sampler_gpu.h:41-42,69-71) is replaced by independent per-query streams.
 #include "launch.h"
 #include "tasks.cuh"
 

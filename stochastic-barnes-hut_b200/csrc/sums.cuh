@@ -18,7 +18,8 @@
 //                    D = -(m + log s) / alpha and its gradient -(g / s) / alpha.
 //
 // Each policy provides: V (the value type), zero(), nan(), add, sub, scale by a
-// float, div by a float, point() and node() (the value of one source record or
+// float, div by a float, warp shuffles of a value (shfl, shfl_up), point() and
+// node() (the value of one source record or
 // node aggregate at query q), and store() (writes the result and, when the
 // caller asks, the gradient as structure-of-arrays [dim][nq]).
 #pragma once
@@ -67,6 +68,12 @@ struct SumF {
   __device__ __forceinline__ static V sub(V a, V b) { return rsub(a, b); }
   __device__ __forceinline__ static V scale(float w, V a) { return rmul(w, a); }
   __device__ __forceinline__ static V div(V a, float d) { return rdiv(a, d); }
+  __device__ __forceinline__ static V shfl(V a, int src) {
+    return __shfl_sync(0xffffffffu, a, src);
+  }
+  __device__ __forceinline__ static V shfl_up(V a, int d) {
+    return __shfl_up_sync(0xffffffffu, a, d);
+  }
   __device__ __forceinline__ static V point(float4 pm, float4 nr, float3 q, const KParams& kp) {
     return kernel_exact<DIM, K>(pm, nr, q, kp);
   }
@@ -106,6 +113,16 @@ struct SumGrad {
   }
   __device__ __forceinline__ static V div(V a, float d) {
     return V{rdiv(a.v, d), a.gx / d, a.gy / d, a.gz / d};
+  }
+  __device__ __forceinline__ static V shfl(V a, int src) {
+    const unsigned f = 0xffffffffu;
+    return V{__shfl_sync(f, a.v, src), __shfl_sync(f, a.gx, src), __shfl_sync(f, a.gy, src),
+             DIM == 3 ? __shfl_sync(f, a.gz, src) : 0.f};
+  }
+  __device__ __forceinline__ static V shfl_up(V a, int d) {
+    const unsigned f = 0xffffffffu;
+    return V{__shfl_up_sync(f, a.v, d), __shfl_up_sync(f, a.gx, d), __shfl_up_sync(f, a.gy, d),
+             DIM == 3 ? __shfl_up_sync(f, a.gz, d) : 0.f};
   }
   __device__ __forceinline__ static V point(float4 pm, float4 nr, float3 q, const KParams& kp) {
     const float v = kernel_exact<DIM, K>(pm, nr, q, kp);
@@ -171,6 +188,16 @@ struct SumLse {
   }
   __device__ __forceinline__ static V div(V a, float d) {
     return V{a.m, a.s / d, a.gx / d, a.gy / d, a.gz / d};
+  }
+  __device__ __forceinline__ static V shfl(V a, int src) {
+    const unsigned f = 0xffffffffu;
+    return V{__shfl_sync(f, a.m, src), __shfl_sync(f, a.s, src), __shfl_sync(f, a.gx, src),
+             __shfl_sync(f, a.gy, src), DIM == 3 ? __shfl_sync(f, a.gz, src) : 0.f};
+  }
+  __device__ __forceinline__ static V shfl_up(V a, int d) {
+    const unsigned f = 0xffffffffu;
+    return V{__shfl_up_sync(f, a.m, d), __shfl_up_sync(f, a.s, d), __shfl_up_sync(f, a.gx, d),
+             __shfl_up_sync(f, a.gy, d), DIM == 3 ? __shfl_up_sync(f, a.gz, d) : 0.f};
   }
   __device__ __forceinline__ static V point(float4 pm, float4, float3 q, const KParams& kp) {
     const float dx = rsub(pm.x, q.x), dy = rsub(pm.y, q.y), dz = DIM == 3 ? rsub(pm.z, q.z) : 0.f;

@@ -122,16 +122,6 @@ __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __re
 
 // ============================================================ sampler ===
 
-constexpr int SBH_VCAP = 512;  // node/child values buffered per warp per pass
-
-// Per-warp shared-memory scratch of the expansion step (V: the policy's value).
-template <class V>
-struct ExpandSmem {
-  V* vals;          // [SBH_VCAP] node and child values of the current pass
-  int* ent;         // [SBH_VCAP] node evaluated at each entry of the current pass
-  unsigned* multi;  // [SBH_VCAP/32] entries that are leaves with several points
-};
-
 // acc += k(point) for every point of leaf tc, in order (rare: leaves with
 // several points exist only for leaf sizes > 1 or at the depth cap).
 template <class A>
@@ -143,58 +133,89 @@ __device__ __forceinline__ typename A::V add_leaf_points(const DevTree& t, int4 
 }
 
 // Expansion of up to 32 internal nodes at once.  Lane l owns node `v` (topo tv)
-// when `own`.  The warp evaluates, as one flat list, every owner's node followed
-// by its children (each owner writes its own entries' node indices, then all
-// lanes evaluate 32 consecutive entries at a time); the owner gets back
-// kv = k(v) and the children sum sum_{children c} k(c) in cell order, leaf
-// children point by point (include/tree_sampler.h:264-280), and `contribs`, the
-// number of kernel evaluations that sum stands for.  All lanes must call.
+// when `own`.  The warp lays every owner's node and its children out as one
+// flat list of entries (owner by owner, each node followed by its children in
+// cell order) and walks it 32 entries at a time: lane r finds the owner of
+// entry r by a binary search over the owners' prefix counts (shuffles), loads
+// that node record (consecutive children: coalesced) and evaluates it -- a leaf
+// child with several points as the sum of its points
+// (include/tree_sampler.h:264-280).  A segmented inclusive scan across the
+// lanes (one segment per owner) adds each owner's children; the owner takes its
+// segment's total from the segment's last lane, and k(v) from its first.  So
+// the owner gets kv = k(v), the children sum, and `contribs`, the number of
+// kernel evaluations that sum stands for.  The children are added as a
+// balanced tree, not left to right: the result is the same sum to within FP32
+// rounding, and deterministic (it depends only on the query, the tree and the
+// random streams).  All lanes must call.
 template <class A>
 __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int v, int4 tv,
-                                                float3 q, const KParams& kp,
-                                                const ExpandSmem<typename A::V>& sm, int lane,
+                                                float3 q, const KParams& kp, int lane,
                                                 typename A::V& kv, int& contribs) {
+  using V = typename A::V;
+  const unsigned full = 0xffffffffu;
   const int nent = own ? tv.y + 1 : 0;
   int incl = nent;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    const int y = __shfl_up_sync(full, incl, o);
     if (lane >= o) incl += y;
   }
   const int excl = incl - nent;
-  const int total = __shfl_sync(0xffffffffu, incl, 31);
-  typename A::V acc = A::zero();
+  const int total = __shfl_sync(full, incl, 31);
+  V acc = A::zero();
   kv = A::zero();
   contribs = 0;
-  for (int base = 0; base < total; base += SBH_VCAP) {
-    const int end = min(total, base + SBH_VCAP);
-    const int s0 = max(excl, base), s1 = min(excl + nent, end);
-    for (int p = s0; p < s1; p++) sm.ent[p - base] = p == excl ? v : tv.x + (p - excl - 1);
-    if (lane < SBH_VCAP / 32) sm.multi[lane] = 0u;
-    __syncwarp();
-    for (int r = lane; r < end - base; r += 32) {
-      // Node record: an aggregate, or for a one-point leaf the point itself.
-      const int c = sm.ent[r];
-      const int4 tc = __ldg(t.nd_topo + c);
-      const float4 cm = __ldg(t.nd_cm + c), ag = __ldg(t.nd_agg + c);
-      if (tc.y == 0 && tc.w - tc.z != 1) atomicOr(sm.multi + (r >> 5), 1u << (r & 31));
-      sm.vals[r] = A::node(cm, ag, q, kp);
+  for (int base = 0; base < total; base += 32) {
+    const int e = base + lane;
+    // owner of entry e: the number of lanes whose inclusive count is <= e
+    int o = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const int c = __shfl_sync(full, incl, o + step - 1);
+      if (c <= e) o += step;
     }
-    __syncwarp();
-    for (int p = s0; p < s1; p++) {
-      const int r = p - base;
-      if (p == excl) {
-        kv = sm.vals[r];
-      } else if ((sm.multi[r >> 5] >> (r & 31)) & 1u) {
-        const int4 tc = __ldg(t.nd_topo + tv.x + (p - excl - 1));
-        acc = add_leaf_points<A>(t, tc, q, kp, acc);
-        contribs += tc.w - tc.z;
+    const int o_excl = __shfl_sync(full, excl, o);
+    const int o_v = __shfl_sync(full, v, o);
+    const int o_first = __shfl_sync(full, tv.x, o);
+    const int k = e - o_excl;  // 0: the owner's node; 1..: its children
+    V val = A::zero();
+    int cnt = 0;
+    if (e < total) {
+      const int node = k == 0 ? o_v : o_first + k - 1;
+      const int4 tc = __ldg(t.nd_topo + node);
+      if (k > 0 && tc.y == 0 && tc.w - tc.z != 1) {
+        val = add_leaf_points<A>(t, tc, q, kp, A::zero());
+        cnt = tc.w - tc.z;
       } else {
-        acc = A::add(acc, sm.vals[r]);
-        contribs += 1;
+        // Node record: an aggregate, or for a one-point leaf the point itself.
+        val = A::node(__ldg(t.nd_cm + node), __ldg(t.nd_agg + node), q, kp);
+        cnt = k > 0 ? 1 : 0;
       }
     }
-    __syncwarp();
+    // Segmented inclusive scan of the children's values (the node's own entry
+    // contributes zero); segment head: the owner's first entry in this chunk.
+    const int head = max(o_excl - base, 0);
+    V x = k > 0 ? val : A::zero();
+    int cx = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const V y = A::shfl_up(x, d);
+      const int cy = __shfl_up_sync(full, cx, d);
+      if (lane - d >= head) {
+        x = A::add(y, x);
+        cx += cy;
+      }
+    }
+    const bool mine = own && excl < base + 32 && incl > base;
+    const int tail = mine ? min(incl, base + 32) - 1 - base : lane;
+    const V part = A::shfl(x, tail);
+    const int pc = __shfl_sync(full, cx, tail);
+    const V node_val = A::shfl(val, mine ? max(excl - base, 0) : lane);
+    if (mine) {
+      acc = A::add(acc, part);
+      contribs += pc;
+      if (excl >= base) kv = node_val;
+    }
   }
   return acc;
 }
@@ -242,12 +263,11 @@ struct SbhWarpSmem {
   V* diffS;       // [R] first-step difference of each subdomain
   int* ccS;       // [R] contributions of that difference
   V* pathv;       // [32] per-path corrections of the current round
-  ExpandSmem<V> ex;
 };
 
 template <class V>
 __host__ __device__ constexpr int sbh_warp_words(int R) {
-  return (int)(sizeof(V) / 4) * (2 * R + 32 + SBH_VCAP) + R + SBH_VCAP + SBH_VCAP / 32;
+  return (int)(sizeof(V) / 4) * (2 * R + 32) + R;
 }
 
 template <class V>
@@ -257,9 +277,6 @@ __device__ __forceinline__ SbhWarpSmem<V> sbh_carve(float* base, int R) {
   w.diffS = w.bhS + R;
   w.ccS = reinterpret_cast<int*>(w.diffS + R);
   w.pathv = reinterpret_cast<V*>(w.ccS + R);
-  w.ex.vals = w.pathv + 32;
-  w.ex.ent = reinterpret_cast<int*>(w.ex.vals + SBH_VCAP);
-  w.ex.multi = reinterpret_cast<unsigned*>(w.ex.ent + SBH_VCAP);
   return w;
 }
 
@@ -296,7 +313,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     const bool own = have && tS.y != 0;
     int cc;
     V kS;
-    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, ws.ex, lane, kS, cc);
+    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, lane, kS, cc);
     if (have) {
       ws.bhS[j] = kS;
       ws.diffS[j] = own ? A::sub(sumc, kS) : A::zero();
@@ -373,7 +390,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       }
       int cc;
       V kprev;
-      const V sumc = expand<A>(t, own, prev, tprev, q, kp, ws.ex, lane, kprev, cc);
+      const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, kprev, cc);
       if (own) {
         wd = A::add(wd, A::scale(w, A::sub(sumc, kprev)));
         cnt += cc;

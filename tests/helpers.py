@@ -13,6 +13,20 @@ def bits_equal(a, b):
     return np.array_equal(a, b)
 
 
+def sampler_close(v, rv, scale, rtol=2e-5):
+    """The GPU sampler against the oracle's estimator on the same Philox paths.
+    Both take the same terms; the GPU adds each node's children as a balanced
+    tree, the oracle left to right, so they differ by rounding: at most a few
+    ulp of `scale`, the magnitude of everything the estimate sums (orc_sbh's
+    scales).  NaN where the oracle has NaN."""
+    v = np.asarray(v, np.float64)
+    rv = np.asarray(rv, np.float64)
+    nan = np.isnan(rv)
+    if not np.array_equal(np.isnan(v), nan):
+        return False
+    return bool(np.all(np.abs(v[~nan] - rv[~nan]) <= rtol * np.asarray(scale)[~nan] + 1e-30))
+
+
 def tree_mismatches(nodes, points, g):
     """Fields of a product tree export that differ (bitwise) from a golden record."""
     bad = []

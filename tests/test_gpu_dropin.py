@@ -8,7 +8,7 @@ import sbh
 import sbh_capi as C
 import sbh_gpu
 import sbh_workloads as W
-from helpers import bits_equal
+from helpers import bits_equal, sampler_close
 
 pytestmark = pytest.mark.gpu
 
@@ -59,8 +59,8 @@ def test_cpu_named_functions_run_on_gpu(torus):
     assert s.shape == (300,) and counts.dtype == np.int32 and (counts > 0).all()
     ot = O.OracleTree(pts, nrm, a, lo, hi, dim_split_log=2)
     assert bits_equal(v, ot.bh(O.GRAVITY, q, 2.0)[0])
-    rs, rc = ot.sbh(O.GRAVITY, q, 2, rng=O.RNG_PHILOX, seed=0)
-    assert bits_equal(s, rs) and np.array_equal(counts, rc)
+    rs, rc, sc = ot.sbh(O.GRAVITY, q, 2, rng=O.RNG_PHILOX, seed=0, return_scale=True)
+    assert sampler_close(s, rs, sc) and np.array_equal(counts, rc)
 
 
 def test_extended_keywords(torus):
