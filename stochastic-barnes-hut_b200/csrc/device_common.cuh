@@ -16,6 +16,7 @@ namespace sbh {
 //           nd_topo[nn] int4   (first child, #children (0 = leaf), start, end)
 //           nd_bmin/nd_bmax [nn] float4 AABB corners (sampler only)
 //           nd_mask[nn][mw] uint64 child-cell bitmask       (sampler only)
+//   points  pt_code[n] uint64 path code (cells per level)   (sampler only)
 // Children of a node are contiguous in buffer order and sorted by cell, so
 // the child in cell c is first_child + popcount(mask bits below c).
 struct DevTree {
@@ -27,9 +28,14 @@ struct DevTree {
   const float4* __restrict__ nd_bmin;
   const float4* __restrict__ nd_bmax;
   const unsigned long long* __restrict__ nd_mask;
+  // Per point, the cell the build assigned it at each level, code_bits bits
+  // per level from level 0 up (code_levels levels fit); bit 63 set: use the
+  // geometric containedInChild test for this point (sampler only).
+  const unsigned long long* __restrict__ pt_code;
   long long n, nn;
   int dim, dsl, ds, bf, mw;
   int depth;          // deepest level
+  int code_bits, code_levels;
   int root_children;  // children of node 0 (0 when the root is a leaf)
   float alpha;        // the tree's smooth-distance alpha
 };

@@ -272,6 +272,10 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
   const size_t o_topo = take(nn * sizeof(int4));
   const size_t o_bmin = take(nn * sizeof(float4)), o_bmax = take(nn * sizeof(float4));
   const size_t o_mask = take((size_t)nn * mw * sizeof(uint64_t));
+  std::vector<uint64_t> pt_code;
+  int code_bits = 0, code_levels = 0;
+  sbh::compute_path_codes(h, pt_code, &code_bits, &code_levels);
+  const size_t o_code = take(n * sizeof(uint64_t));
 
   sbh_gpu_tree* g = new (std::nothrow) sbh_gpu_tree();
   if (!g) return sbh::fail(SBH_ERR_OUT_OF_MEMORY, "host allocation failed");
@@ -295,7 +299,8 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
                 {o_topo, nd_topo.data(), nn * sizeof(int4)},
                 {o_bmin, nd_bmin.data(), nn * sizeof(float4)},
                 {o_bmax, nd_bmax.data(), nn * sizeof(float4)},
-                {o_mask, h.mask.data(), (size_t)nn * mw * sizeof(uint64_t)}};
+                {o_mask, h.mask.data(), (size_t)nn * mw * sizeof(uint64_t)},
+                {o_code, pt_code.data(), n * sizeof(uint64_t)}};
   e = cudaMemset(base + o_status, 0, sizeof(int));
   for (const Copy& c : copies)
     if (e == cudaSuccess && c.bytes) e = cudaMemcpy(base + c.off, c.src, c.bytes, cudaMemcpyHostToDevice);
@@ -317,6 +322,9 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
   t.nd_bmin = reinterpret_cast<const float4*>(base + o_bmin);
   t.nd_bmax = reinterpret_cast<const float4*>(base + o_bmax);
   t.nd_mask = reinterpret_cast<const unsigned long long*>(base + o_mask);
+  t.pt_code = reinterpret_cast<const unsigned long long*>(base + o_code);
+  t.code_bits = code_bits;
+  t.code_levels = code_levels;
   t.n = n;
   t.nn = nn;
   t.dim = d;

@@ -288,4 +288,42 @@ void build_host_tree(HostTree& t, int dim, int dsl, int leaf_size, int max_depth
   }
 }
 
+void compute_path_codes(const HostTree& t, std::vector<uint64_t>& code, int* bits_out,
+                        int* levels_out) {
+  const int dim = t.dim, bits = dim * t.dsl, levels = 63 / bits;
+  *bits_out = bits;
+  *levels_out = levels;
+  code.assign(static_cast<size_t>(t.n), 0);
+  const int64_t nn = t.nn;
+  // Cell of every node under its parent: the k-th set bit of the parent's mask
+  // is the cell of its k-th child.
+  std::vector<uint16_t> ncell(static_cast<size_t>(nn), 0);
+  for (int64_t v = 0; v < nn; v++) {
+    if (t.leaf[v]) continue;
+    int64_t k = 0;
+    for (int c = 0; c < t.bf; c++)
+      if ((t.mask[v * t.mw + (c >> 6)] >> (c & 63)) & 1u)
+        ncell[t.first_child[v] + k++] = static_cast<uint16_t>(c);
+  }
+  parallel_for(nn, 256, [&](int64_t v) {
+    if (!t.leaf[v]) return;
+    uint64_t c = 0;
+    for (int64_t u = v; u != 0; u = t.parent[u]) {
+      const int dp = t.node_depth[t.parent[u]];
+      if (dp < levels) c |= static_cast<uint64_t>(ncell[u]) << (bits * dp);
+    }
+    for (int64_t i = t.start[v]; i < t.end[v]; i++) {
+      const float* p = &t.pos[i * dim];
+      bool ok = true;
+      for (int64_t a = t.parent[v]; ok && a != 0; a = t.parent[a]) {
+        for (int k = 0; k < dim; k++) {
+          const float lo = t.bmin[a * dim + k] - 1e-4f, hi = t.bmax[a * dim + k] + 1e-4f;
+          if (!(lo <= p[k] && p[k] <= hi)) ok = false;
+        }
+      }
+      code[i] = ok ? c : (c | (uint64_t(1) << 63));
+    }
+  });
+}
+
 }  // namespace sbh

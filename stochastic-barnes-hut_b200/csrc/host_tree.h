@@ -47,4 +47,14 @@ void build_host_tree(HostTree& t, int dim, int dim_split_log, int leaf_size, int
                      const float* points, const float* normals, const float* masses, int64_t n,
                      const float* min_corner, const float* max_corner, float alpha);
 
+// Path codes of the points (build order): for the point's ancestor at depth d
+// (d < levels), bits [bits*d, bits*(d+1)) hold the cell of its depth-(d+1)
+// ancestor under it -- the cell the build's quantize assigned the point there.
+// bits = dim * dim_split_log, levels = 63 / bits.  Bit 63 is set for a point
+// that fails the reference's containedInChild AABB check (1e-4 slack,
+// include/aabb.h:28-32) at one of its internal ancestors of depth >= 1, so
+// that a walk for it takes the geometric test (and reports what the reference
+// would do there).
+void compute_path_codes(const HostTree& t, std::vector<uint64_t>& code, int* bits, int* levels);
+
 }  // namespace sbh

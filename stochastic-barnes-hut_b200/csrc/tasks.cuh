@@ -220,20 +220,39 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
   return acc;
 }
 
-// containedInChild(VectorNd p) (include/tree3d.h:172-183): the child of v whose
-// cell holds p, skipping single-child chains.  A cell without a child reads the
-// root (child_buffer_idxs_ is value-initialised to 0 in the reference).
-// Returns -1 where the reference would return nullptr.
+// containedInChild(VectorNd p) (include/tree3d.h:172-183) for sampled point
+// `idx`: the child of v (at depth dv) whose cell holds the point, skipping
+// single-child chains; *dout receives the depth of the node returned.
+//
+// The cell comes from the point's path code when it holds one: the cells the
+// build assigned the point at every level (upload computes them from the
+// tree), which are exactly what quantizing the point under each ancestor's
+// AABB gives, since the build quantized it the same way.  Points whose code is
+// marked (an ancestor's AABB check would fail) and levels beyond the code fall
+// back to the geometric test: the AABB check with 1e-4 slack, then quantize.
+// A cell without a child reads the root (child_buffer_idxs_ is
+// value-initialised to 0 in the reference).  Returns -1 where the reference
+// would return nullptr.
 template <int DIM>
-__device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 tv, float3 p,
-                                                  int4& tout) {
+__device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 tv, int dv,
+                                                  unsigned long long code, int idx, int4& tout,
+                                                  int& dout) {
+  const bool coded = (code >> 63) == 0ull;
+  const unsigned cell_mask = (1u << t.code_bits) - 1u;
   for (int guard = 0; guard <= t.depth + 1; guard++) {
-    const float4 lo = __ldg(t.nd_bmin + v), hi = __ldg(t.nd_bmax + v);
-    if (!aabb_contains<DIM>(lo, hi, p)) return -1;
-    const int cx = quantize1(p.x, lo.x, hi.x, t.ds);
-    const int cy = quantize1(p.y, lo.y, hi.y, t.ds);
-    const int cz = DIM == 3 ? quantize1(p.z, lo.z, hi.z, t.ds) : 0;
-    const int cell = (((cz << t.dsl) + cy) << t.dsl) + cx;
+    int cell;
+    if (coded && dv < t.code_levels) {
+      cell = (int)((code >> (t.code_bits * dv)) & cell_mask);
+    } else {
+      const float4 sp = __ldg(t.pt_pm + idx);
+      const float3 p = make_float3(sp.x, sp.y, sp.z);
+      const float4 lo = __ldg(t.nd_bmin + v), hi = __ldg(t.nd_bmax + v);
+      if (!aabb_contains<DIM>(lo, hi, p)) return -1;
+      const int cx = quantize1(p.x, lo.x, hi.x, t.ds);
+      const int cy = quantize1(p.y, lo.y, hi.y, t.ds);
+      const int cz = DIM == 3 ? quantize1(p.z, lo.z, hi.z, t.ds) : 0;
+      cell = (((cz << t.dsl) + cy) << t.dsl) + cx;
+    }
     const unsigned long long* m = t.nd_mask + (long long)v * t.mw;
     const int w = cell >> 6, b = cell & 63;
     const unsigned long long word = __ldg(m + w);
@@ -244,8 +263,10 @@ __device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 
       child = tv.x + rank;
     }
     const int4 tc = __ldg(t.nd_topo + child);
+    dv = child == 0 ? 0 : dv + 1;
     if (tc.y != 1) {
       tout = tc;
+      dout = dv;
       return child;
     }
     v = child;
@@ -333,7 +354,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     int j = 0, S = 0, cur = 0;
     int4 tcur = make_int4(0, 0, 0, 0);
     float spi = 0.f, ev = 1.f, cb = 1.f;
-    float3 p = make_float3(0.f, 0.f, 0.f);
+    unsigned long long code = 0ull;  // the sampled point's path code
+    int idx = 0, dcur = 1;           // the sampled point; depth of cur
     PathRng rng;
     if (pid < P) {
       j = pid / samples;
@@ -341,9 +363,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       const int4 tS = __ldg(t.nd_topo + S);
       rng.begin(seed, (unsigned long long)qi, (uint32_t)pid);
       const uint32_t nS = (uint32_t)(tS.w - tS.z);
-      const int idx = tS.z + (int)rng.index(nS);
-      const float4 sp = __ldg(t.pt_pm + idx);
-      p = make_float3(sp.x, sp.y, sp.z);
+      idx = tS.z + (int)rng.index(nS);
+      code = __ldg(t.pt_code + idx);
       spi = (float)nS;
       cur = S;
       tcur = tS;
@@ -369,7 +390,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
           prev = cur;
           tprev = tcur;
           int4 tnext;
-          cur = contained_in_child<DIM>(t, prev, tprev, p, tnext);
+          cur = contained_in_child<DIM>(t, prev, tprev, dcur, code, idx, tnext, dcur);
           if (cur < 0) {
             report_status(status, kStatusNullChild);
             wd = A::nan();
