@@ -701,13 +701,38 @@ def serving_errors(C, trees, reqs, gpus_bf, outs, pick):
     return {k: (float(np.median(np.concatenate(v))) if v else None) for k, v in errs.items()}
 
 
+def serving_tuning(C, W, trees, reqs, gpus, n=256):
+    """Batch schedule for the server, chosen by the autotuner on a representative
+    batch: the first `n` requests of the stream, each once as stochastic BH and
+    once as Barnes-Hut (untimed)."""
+    import torch
+    gpus2 = {}
+    entries, keep = [], []
+    for r in reqs[:n]:
+        t = trees[r["tree"]]
+        if r["tree"] not in gpus2:
+            gpus2[r["tree"]] = C.GpuTree(t["sbh"])
+        dq = torch.from_numpy(np.ascontiguousarray(r["q"].T)).cuda()
+        for method, g in (("sbh", gpus2[r["tree"]]), ("bh", gpus[r["tree"]])):
+            out = torch.empty(r["nq"], dtype=torch.float32, device="cuda")
+            entries.append((g, serving_params(C, W, t, r, method), dq.data_ptr(), r["nq"],
+                            out.data_ptr(), 0, 0))
+            keep.append(out)
+        keep.append(dq)
+    best, best_ms, start_ms = C.batch_autotune(entries, stream=0, repeats=2)
+    torch.cuda.synchronize()
+    return best, {"tuning": best.as_dict(), "tuned_ms": best_ms, "default_ms": start_ms,
+                  "batch": f"first {n} requests, each as stochastic BH and as Barnes-Hut"}
+
+
 def run_serving(args):
     import sbh_capi as C
     import sbh_workloads as W
     t_setup = time.perf_counter()
     trees, reqs = serving_setup(C)
     gpus = {i: C.GpuTree(t["bh"]) for i, t in enumerate(trees)}
-    server = C.Server(slots=3, slot_queries=1 << 20, max_requests_per_batch=4096)
+    tuning, tune_info = serving_tuning(C, W, trees, reqs, gpus)
+    server = C.Server(slots=3, slot_queries=1 << 20, max_requests_per_batch=4096, tuning=tuning)
     ids = {}
     for i, t in enumerate(trees):
         ids[(i, "sbh")] = server.add_tree(t["sbh"])
@@ -763,6 +788,7 @@ def run_serving(args):
                    "requests": len(reqs), "queries": total_q, "setup_s": setup_s,
                    "server": {"slots": 3, "slot_queries": 1 << 20}},
         "serving": results, "server_stats": stats, "clocks": sampler.summary(),
+        "autotune": tune_info,
     }
 
 

@@ -128,8 +128,8 @@ constexpr int kTreeWords = (int)((sizeof(DevTree) + 15) / 16 * 4);
 template <int DIM, int K, bool VOTE>
 __device__ __noinline__ void run_bh(const DevTree& t, const BatchItem& it, long long u,
                                     const int* ord, float* scratch, int stack_cap, int* status) {
-  const long long s0 = u * kUnitQueriesWarp;
-  const long long s1 = min(it.nq, s0 + kUnitQueriesWarp);
+  const long long s0 = u * it.unit_queries;
+  const long long s1 = min(it.nq, s0 + it.unit_queries);
   bh_warp_task<DIM, K, VOTE>(t, it.q, it.nq, ord, s0, s1, it.beta, it.kp, it.out, it.contribs,
                              status, reinterpret_cast<BhStackEntry*>(scratch), stack_cap,
                              it.self_mass);
@@ -285,7 +285,8 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
                               const Tuning& tuning) const {
   if (!dev_ || !h_stage_) return "batch engine has no device or pinned memory";
   if (tuning.sampler_unit < 1 || tuning.sampler_unit > 64 || tuning.bucket_queries < 2 ||
-      tuning.bucket_queries > 4096 || tuning.blocks_per_sm < 0)
+      tuning.bucket_queries > 4096 || tuning.blocks_per_sm < 0 || tuning.bh_unit < 1 ||
+      tuning.bh_unit > 32)
     return "batch tuning out of range";
   if ((int)items.size() > lim_.max_items) return "too many requests in one batch";
   long long sort_base = 0, bucket_base = 0, unit_base = 0;
@@ -302,7 +303,12 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
     it.bucket_base = bucket_base;
     it.buckets = it.sort_bits > 0 ? (1LL << (t.dim * it.sort_bits)) : 1;
     it.unit_base = unit_base;
-    it.unit_queries = it.method == 3 ? tuning.sampler_unit : kUnitQueriesWarp;
+    // Work unit: sampler queries per warp (tuned); Barnes-Hut queries per warp
+    // walk (tuned; vote keeps 32, its acceptance is defined over 32 queries);
+    // brute force 32 queries per warp.
+    it.unit_queries = it.method == 3   ? tuning.sampler_unit
+                      : it.method == 1 ? tuning.bh_unit
+                                       : kUnitQueriesWarp;
     it.units = (it.nq + it.unit_queries - 1) / it.unit_queries;
     sort_base += it.nq;
     bucket_base += it.buckets;

@@ -48,8 +48,9 @@ struct BatchHeader {
   unsigned long long next_unit;  // work counter of the persistent kernel
 };
 
-// Queries per work unit (one warp task) of Barnes-Hut and brute force: 32,
-// a lane each.  The sampler gives each query a warp; its unit size is tuned.
+// Queries per work unit (one warp task) of brute force: 32, a lane each.  The
+// sampler gives each query a warp and Barnes-Hut a lane; their unit sizes
+// (queries per warp task) are tuned.
 constexpr int kUnitQueriesWarp = 32;
 
 class BatchEngine {
@@ -59,6 +60,7 @@ class BatchEngine {
     int sampler_unit = 2;     // sampler queries per work unit
     int bucket_queries = 8;   // target queries per Morton bucket
     int blocks_per_sm = 0;    // persistent CTAs per SM (0: as many as fit)
+    int bh_unit = 32;         // Barnes-Hut queries per warp walk (1..32)
   };
 
   struct Limits {

@@ -9,7 +9,8 @@ namespace sbh {
 // Device image of a tree.  Arrays are structure-of-arrays in HBM:
 //   points  pt_pm  [n]  float4 (x, y, z, mass)        z = 0 in 2D
 //           pt_nrm [n]  float4 (nx, ny, nz, 0)
-//   nodes   nd_cm  [nn] float4 (centroid x, y, z, diameter)
+//   nodes   nd_cm  [nn] float4 (centroid x, y, z, diameter; -1 for a leaf
+//                               holding more or fewer than one point)
 //           nd_agg [nn] float4 (mass, normal x, y, z)      aggregate LeafData
 //           (a leaf holding exactly one point stores that point's position,
 //           mass and normal instead of its aggregate)

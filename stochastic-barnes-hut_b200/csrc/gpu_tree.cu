@@ -251,7 +251,12 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
       nd_cm[v] = make_float4(h.pos[i * d], h.pos[i * d + 1], d == 3 ? h.pos[i * d + 2] : 0.f, h.diam[v]);
       nd_agg[v] = make_float4(h.mass[i], h.nrm[i * d], h.nrm[i * d + 1], d == 3 ? h.nrm[i * d + 2] : 0.f);
     } else {
-      nd_cm[v] = make_float4(h.apos[v * d], h.apos[v * d + 1], d == 3 ? h.apos[v * d + 2] : 0.f, h.diam[v]);
+      // A leaf with several points (or none) marks itself by a negative
+      // diameter, which no walk reads for a leaf (a leaf's far-field ratio is
+      // infinite): the sampler's expansions then need not load its topology to
+      // know that its points must be summed.
+      const float w = h.leaf[v] ? -1.0f : h.diam[v];
+      nd_cm[v] = make_float4(h.apos[v * d], h.apos[v * d + 1], d == 3 ? h.apos[v * d + 2] : 0.f, w);
       nd_agg[v] = make_float4(h.amass[v], h.anrm[v * d], h.anrm[v * d + 1], d == 3 ? h.anrm[v * d + 2] : 0.f);
     }
     nd_bmin[v] = make_float4(h.bmin[v * d], h.bmin[v * d + 1], d == 3 ? h.bmin[v * d + 2] : 0.f, 0.f);

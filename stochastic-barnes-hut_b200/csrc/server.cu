@@ -106,6 +106,7 @@ BatchEngine::Tuning to_engine(const sbh_batch_tuning& t) {
   e.sampler_unit = t.sampler_unit_queries;
   e.bucket_queries = t.bucket_queries;
   e.blocks_per_sm = t.blocks_per_sm;
+  e.bh_unit = t.bh_unit_queries;
   return e;
 }
 
@@ -114,6 +115,7 @@ sbh_batch_tuning from_engine(const BatchEngine::Tuning& e) {
   t.sampler_unit_queries = e.sampler_unit;
   t.bucket_queries = e.bucket_queries;
   t.blocks_per_sm = e.blocks_per_sm;
+  t.bh_unit_queries = e.bh_unit;
   return t;
 }
 
@@ -125,6 +127,8 @@ int check_tuning(const sbh_batch_tuning* t) {
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "bucket_queries must be in [2, 4096]");
   if (t->blocks_per_sm < 0 || t->blocks_per_sm > 64)
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "blocks_per_sm must be in [0, 64]");
+  if (t->bh_unit_queries < 1 || t->bh_unit_queries > 32)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "bh_unit_queries must be in [1, 32]");
   return SBH_OK;
 }
 
@@ -335,7 +339,7 @@ SBH_API int sbh_batch_autotune(const sbh_batch_item* items, int n_items, void* s
   const float first_ms = cur_ms;
   // Coordinate descent; a candidate must win by 2% to replace the incumbent.
   const int max_bps = ctx.engine ? ctx.engine->max_blocks_per_sm() : 1;
-  for (int coord = 0; coord < 3 && st == SBH_OK; coord++) {
+  for (int coord = 0; coord < 4 && st == SBH_OK; coord++) {
     std::vector<int> values;
     if (coord == 0) {
       for (int v : {0, max_bps * 3 / 4, max_bps / 2, max_bps / 4})
@@ -344,14 +348,19 @@ SBH_API int sbh_batch_autotune(const sbh_batch_item* items, int n_items, void* s
           values.push_back(v);
     } else if (coord == 1) {
       values = {1, 2, 4, 8};
-    } else {
+    } else if (coord == 2) {
       values = {4, 8, 16, 32};
+    } else {
+      values = {32, 16, 8};
     }
     BatchEngine::Tuning best_t = cur;
     float best_t_ms = cur_ms;
     for (int v : values) {
       BatchEngine::Tuning t = cur;
-      int& field = coord == 0 ? t.blocks_per_sm : coord == 1 ? t.sampler_unit : t.bucket_queries;
+      int& field = coord == 0   ? t.blocks_per_sm
+                   : coord == 1 ? t.sampler_unit
+                   : coord == 2 ? t.bucket_queries
+                                : t.bh_unit;
       if (field == v) continue;
       field = v;
       float ms = 0.f;

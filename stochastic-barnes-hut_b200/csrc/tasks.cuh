@@ -150,7 +150,7 @@ __device__ __forceinline__ typename A::V add_leaf_points(const DevTree& t, int4 
 template <class A>
 __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int v, int4 tv,
                                                 float3 q, const KParams& kp, int lane,
-                                                typename A::V& kv, int& contribs) {
+                                                int* ownlane, typename A::V& kv, int& contribs) {
   using V = typename A::V;
   const unsigned full = 0xffffffffu;
   const int nent = own ? tv.y + 1 : 0;
@@ -162,18 +162,21 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
   }
   const int excl = incl - nent;
   const int total = __shfl_sync(full, incl, 31);
+  // Owners in lane order: ownlane[r] is the lane of the r-th owner.
+  const unsigned owners = __ballot_sync(full, own);
+  if (own) ownlane[__popc(owners & ((1u << lane) - 1u))] = lane;
+  __syncwarp();
   V acc = A::zero();
   kv = A::zero();
   contribs = 0;
   for (int base = 0; base < total; base += 32) {
     const int e = base + lane;
-    // owner of entry e: the number of lanes whose inclusive count is <= e
-    int o = 0;
-#pragma unroll
-    for (int step = 16; step > 0; step >>= 1) {
-      const int c = __shfl_sync(full, incl, o + step - 1);
-      if (c <= e) o += step;
-    }
+    // Owner of entry e: the owner whose segment covers the chunk's first entry,
+    // advanced by the segments that start between there and e.
+    const unsigned starts =
+        __reduce_or_sync(full, (own && excl >= base && excl < base + 32) ? 1u << (excl - base) : 0u);
+    const int first = __popc(__ballot_sync(full, own && excl <= base)) - 1;
+    const int o = ownlane[min(first + __popc(starts & (((2u << lane) - 1u) & ~1u)), 31)];
     const int o_excl = __shfl_sync(full, excl, o);
     const int o_v = __shfl_sync(full, v, o);
     const int o_first = __shfl_sync(full, tv.x, o);
@@ -182,13 +185,16 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
     int cnt = 0;
     if (e < total) {
       const int node = k == 0 ? o_v : o_first + k - 1;
-      const int4 tc = __ldg(t.nd_topo + node);
-      if (k > 0 && tc.y == 0 && tc.w - tc.z != 1) {
+      // Node record: an aggregate, or for a one-point leaf the point itself; a
+      // negative diameter marks a leaf whose points must be summed.
+      const float4 cm = __ldg(t.nd_cm + node);
+      const float4 ag = __ldg(t.nd_agg + node);
+      if (k > 0 && cm.w < 0.f) {
+        const int4 tc = __ldg(t.nd_topo + node);
         val = add_leaf_points<A>(t, tc, q, kp, A::zero());
         cnt = tc.w - tc.z;
       } else {
-        // Node record: an aggregate, or for a one-point leaf the point itself.
-        val = A::node(__ldg(t.nd_cm + node), __ldg(t.nd_agg + node), q, kp);
+        val = A::node(cm, ag, q, kp);
         cnt = k > 0 ? 1 : 0;
       }
     }
@@ -284,11 +290,12 @@ struct SbhWarpSmem {
   V* diffS;       // [R] first-step difference of each subdomain
   int* ccS;       // [R] contributions of that difference
   V* pathv;       // [32] per-path corrections of the current round
+  int* ownlane;   // [32] lanes of the current expansion's owners, in order
 };
 
 template <class V>
 __host__ __device__ constexpr int sbh_warp_words(int R) {
-  return (int)(sizeof(V) / 4) * (2 * R + 32) + R;
+  return (int)(sizeof(V) / 4) * (2 * R + 32) + R + 32;
 }
 
 template <class V>
@@ -298,6 +305,7 @@ __device__ __forceinline__ SbhWarpSmem<V> sbh_carve(float* base, int R) {
   w.diffS = w.bhS + R;
   w.ccS = reinterpret_cast<int*>(w.diffS + R);
   w.pathv = reinterpret_cast<V*>(w.ccS + R);
+  w.ownlane = reinterpret_cast<int*>(w.pathv + 32);
   return w;
 }
 
@@ -334,7 +342,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     const bool own = have && tS.y != 0;
     int cc;
     V kS;
-    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, lane, kS, cc);
+    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, lane, ws.ownlane, kS, cc);
     if (have) {
       ws.bhS[j] = kS;
       ws.diffS[j] = own ? A::sub(sumc, kS) : A::zero();
@@ -411,7 +419,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       }
       int cc;
       V kprev;
-      const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, kprev, cc);
+      const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, ws.ownlane, kprev, cc);
       if (own) {
         wd = A::add(wd, A::scale(w, A::sub(sumc, kprev)));
         cnt += cc;

@@ -97,11 +97,12 @@ class BatchItem(ctypes.Structure):
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("sampler_unit_queries", ctypes.c_int32), ("bucket_queries", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_int32), ("bh_unit_queries", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {"sampler_unit_queries": self.sampler_unit_queries,
-                "bucket_queries": self.bucket_queries, "blocks_per_sm": self.blocks_per_sm}
+                "bucket_queries": self.bucket_queries, "blocks_per_sm": self.blocks_per_sm,
+                "bh_unit_queries": self.bh_unit_queries}
 
 
 class ServerConfig(ctypes.Structure):
@@ -331,7 +332,8 @@ def eval_batch(entries, stream: int = 0):
     _check(lib().sbh_eval_batch(_batch_items(entries), len(entries), ctypes.c_void_p(stream)))
 
 
-def batch_tuning(sampler_unit_queries=None, bucket_queries=None, blocks_per_sm=None) -> BatchTuning:
+def batch_tuning(sampler_unit_queries=None, bucket_queries=None, blocks_per_sm=None,
+                 bh_unit_queries=None) -> BatchTuning:
     """A tuning with the library defaults, overridden where given."""
     t = BatchTuning()
     lib().sbh_batch_tuning_init(ctypes.byref(t))
@@ -341,6 +343,8 @@ def batch_tuning(sampler_unit_queries=None, bucket_queries=None, blocks_per_sm=N
         t.bucket_queries = bucket_queries
     if blocks_per_sm is not None:
         t.blocks_per_sm = blocks_per_sm
+    if bh_unit_queries is not None:
+        t.bh_unit_queries = bh_unit_queries
     return t
 
 

@@ -184,7 +184,9 @@ def test_batch_results_do_not_depend_on_tuning(env):
     outs = []
     try:
         for t in (C.batch_tuning(), C.batch_tuning(sampler_unit_queries=1, bucket_queries=32),
-                  C.batch_tuning(sampler_unit_queries=8, bucket_queries=2, blocks_per_sm=1)):
+                  C.batch_tuning(sampler_unit_queries=8, bucket_queries=2, blocks_per_sm=1,
+                                 bh_unit_queries=8),
+                  C.batch_tuning(bh_unit_queries=3)):
             C.set_batch_tuning(t)
             for _, out, _ in keep:
                 out.zero_()
@@ -200,6 +202,8 @@ def test_batch_results_do_not_depend_on_tuning(env):
         C.set_batch_tuning(C.batch_tuning(sampler_unit_queries=0))
     with pytest.raises(C.SbhError):
         C.set_batch_tuning(C.batch_tuning(bucket_queries=1))
+    with pytest.raises(C.SbhError):
+        C.set_batch_tuning(C.batch_tuning(bh_unit_queries=33))
 
 
 def test_autotune_installs_a_valid_tuning(env):
@@ -211,7 +215,7 @@ def test_autotune_installs_a_valid_tuning(env):
         best, best_ms, start_ms = C.batch_autotune(entries, stream=stream, repeats=2)
         assert 0 < best_ms <= start_ms
         assert 1 <= best.sampler_unit_queries <= 64 and 2 <= best.bucket_queries <= 4096
-        assert best.blocks_per_sm >= 0
+        assert best.blocks_per_sm >= 0 and 1 <= best.bh_unit_queries <= 32
         assert C.get_batch_tuning().as_dict() == best.as_dict()
         # the buffers hold the batch's results
         torch.cuda.synchronize()
