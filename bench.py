@@ -982,6 +982,8 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=4096)
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
     ap.add_argument("--nq", type=int, default=0, help="override the query count (profiling)")
+    ap.add_argument("--budget", type=int, default=0,
+                    help="override the sampled paths per query of a stochastic workload")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -996,6 +998,9 @@ def main():
     if args.nq:
         wl["nq"] = args.nq
         wl["desc"] += f" [query count overridden: {args.nq}]"
+    if args.budget and wl["method"] == "stochastic":
+        wl["budget"] = args.budget
+        wl["desc"] += f" [budget overridden: {args.budget} paths/query]"
     out = run_reference(args, wl) if args.impl == "reference" else run_ours(args, wl)
     if out is not None:
         print(json.dumps(out), flush=True)
