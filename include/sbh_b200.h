@@ -129,6 +129,14 @@ int sbh_host_tree_export_nodes(const sbh_host_tree* tree, int64_t* start, int64_
 int sbh_host_tree_export_points(const sbh_host_tree* tree, float* points, float* normals,
                                 float* masses);
 
+/* Serialisation (no counterpart in the reference, which rebuilds its trees in
+ * every process).  A file holds the whole tree -- points in build order, every
+ * node array, aggregates -- and a checksum; loading verifies the checksum and
+ * the tree's structure and returns SBH_ERR_INVALID_ARGUMENT for a damaged or
+ * foreign file.  A loaded tree equals the saved one bit for bit. */
+int sbh_host_tree_save(const sbh_host_tree* tree, const char* path);
+int sbh_host_tree_load(const char* path, sbh_host_tree** out);
+
 /* ---- device-resident trees --------------------------------------------------
  * Uploads a host tree to `device` in structure-of-arrays form.  Replaces
  * PyQuadtreeGPU/PyOctreeGPU's constructor (include/py_tree_gpu.h:38-49, 69-80).

@@ -64,6 +64,8 @@ _SIGNATURES = {
     "sbh_eval_grad": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _P]),
     "sbh_eval_grad_device": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P]),
     "sbh_measure_pipe_rates": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P]),
+    "sbh_host_tree_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "sbh_host_tree_load": (ctypes.c_int, [ctypes.c_char_p, _P]),
     "sbh_batch_tuning_init": (None, [_P]),
     "sbh_batch_set_tuning": (ctypes.c_int, [ctypes.c_int, _P]),
     "sbh_batch_get_tuning": (ctypes.c_int, [ctypes.c_int, _P]),
@@ -189,6 +191,19 @@ class HostTree:
         i = TreeInfo()
         _check(lib().sbh_host_tree_info(self.handle, ctypes.byref(i)))
         return i
+
+    def save(self, path: str):
+        """sbh_host_tree_save: the whole tree to a file."""
+        _check(lib().sbh_host_tree_save(self.handle, os.fsencode(path)))
+
+    @classmethod
+    def load(cls, path: str) -> "HostTree":
+        """sbh_host_tree_load: a tree saved by save(), verified."""
+        h = ctypes.c_void_p()
+        _check(lib().sbh_host_tree_load(os.fsencode(path), ctypes.byref(h)))
+        t = cls.__new__(cls)
+        t.handle = h
+        return t
 
     def export_nodes(self) -> dict:
         i = self.info()

@@ -279,3 +279,19 @@ def test_invalid_requests_are_rejected():
     # The tree stays usable after rejected calls.
     v, _ = gpu.eval(g["queries"], C.params(method=C.BARNES_HUT, kernel=C.GRAVITY))
     assert bits_equal(v, g["bh_k0_b2.0"])
+
+
+def test_loaded_tree_evaluates_identically(tmp_path):
+    """A tree saved and loaded (sbh_host_tree_save/load) uploads and evaluates
+    exactly as the tree it was saved from."""
+    pts, nrm, a = W.torus_surface(20000, seed=29)
+    lo, hi = W.padded_box(pts)
+    t = C.HostTree(pts, nrm, a, lo, hi, dim_split_log=2)
+    t.save(str(tmp_path / "t.sbht"))
+    u = C.HostTree.load(str(tmp_path / "t.sbht"))
+    g1, g2 = C.GpuTree(t), C.GpuTree(u)
+    q = W.uniform_queries(3000, seed=30)
+    for p in (C.params(method=C.BARNES_HUT, kernel=C.WINDING_NUMBER, beta=2.0),
+              C.params(method=C.STOCHASTIC, kernel=C.WINDING_NUMBER, samples_per_subdomain=2,
+                       seed=4)):
+        assert bits_equal(g1.eval(q, p)[0], g2.eval(q, p)[0])

@@ -11,7 +11,7 @@ import sbh
 import sbh_capi as C
 import sbh_workloads as W
 from conftest import golden_cases, load_golden
-from helpers import tree_mismatches
+from helpers import bits_equal, tree_mismatches
 
 NAMED = {(2, 1): sbh.Quadtree1, (2, 2): sbh.Quadtree2, (2, 3): sbh.Quadtree3,
          (3, 1): sbh.Octree1, (3, 2): sbh.Octree2, (3, 3): sbh.Octree3}
@@ -105,3 +105,48 @@ def test_large_torus_build_is_deterministic():
     e1, e2 = t1.export_nodes(), t2.export_nodes()
     for k in e1:
         assert np.array_equal(e1[k], e2[k]), k
+
+
+# ------------------------------------------------------------ serialisation
+
+def test_save_load_roundtrip_is_bit_identical(tmp_path):
+    pts, nrm, m = W.torus_surface(5000, seed=17)
+    lo, hi = W.padded_box(pts)
+    for dsl, leaf in ((1, 1), (2, 1), (1, 8)):
+        t = C.HostTree(pts, nrm, m, lo, hi, alpha=3.5, dim_split_log=dsl, leaf_size=leaf)
+        path = str(tmp_path / f"tree_{dsl}_{leaf}.sbht")
+        t.save(path)
+        u = C.HostTree.load(path)
+        a, b = t.export_nodes(), u.export_nodes()
+        for k in a:
+            assert bits_equal(a[k], b[k]), k
+        pa, pb = t.export_points(), u.export_points()
+        for k in pa:
+            assert bits_equal(pa[k], pb[k]), k
+        ia, ib = t.info(), u.info()
+        assert (ia.num_nodes, ia.depth, ia.root_children, ia.alpha) == \
+            (ib.num_nodes, ib.depth, ib.root_children, ib.alpha)
+
+
+def test_load_rejects_damaged_files(tmp_path):
+    pts, nrm, m = W.gaussian_mixture(2000, seed=18)
+    lo, hi = W.padded_box(pts)
+    t = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=2)
+    path = tmp_path / "t.sbht"
+    t.save(str(path))
+    raw = bytearray(path.read_bytes())
+    bad = tmp_path / "bad.sbht"
+    for damage in ("flip", "truncate", "magic"):
+        b = bytearray(raw)
+        if damage == "flip":
+            b[len(b) // 2] ^= 0x40
+        elif damage == "truncate":
+            b = b[: len(b) - 100]
+        else:
+            b[0:4] = b"XXXX"
+        bad.write_bytes(bytes(b))
+        with pytest.raises(C.SbhError) as e:
+            C.HostTree.load(str(bad))
+        assert e.value.status == C.ERR_INVALID_ARGUMENT
+    with pytest.raises(C.SbhError):
+        C.HostTree.load(str(tmp_path / "missing.sbht"))
