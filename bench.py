@@ -9,7 +9,8 @@ budget of 256 sampled paths per query (samples_per_subdomain = 256 / root
 children).  A step is one evaluation of all queries.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sbh_wn|bh_wn|plain_small_bf|plain_small_bh]
+                    [--workload sbh_wn|bh_wn|plain_small_bf|plain_small_bh|differentiation|
+                                batching|serving|tree_build] [--nq N] [--budget B]
 
 `value` is queries/s with queries already resident in HBM (device-pointer C ABI
 call: Morton bucketing + sampler kernel), timed with CUDA events per step, L2
@@ -967,6 +968,63 @@ def run_differentiation(args):
     }
 
 
+# -------------------------------------------------------------- tree build
+
+def run_tree_build(args):
+    """Tree construction, 1,048,576 torus points, Octree2 and Octree1 (leaf 1):
+    the GPU build (sbh_gpu_tree_build) against the host build + upload and the
+    reference's own build (src/sbh.cpp's Octree constructors, compiled in
+    oracle/_ref), all producing the same tree."""
+    import torch
+
+    import sbh_capi as C
+    import sbh_workloads as W
+    pts, nrm, a = W.torus_surface(1 << 20, seed=2024)
+    lo, hi = W.padded_box(pts)
+    res = {}
+    for dsl in (2, 1):
+        C.GpuTree.build(pts[:4096], nrm[:4096], a[:4096], lo, hi, dim_split_log=dsl)  # warm-up
+        gpu_s = []
+        for _ in range(max(3, args.steps // 4)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            g = C.GpuTree.build(pts, nrm, a, lo, hi, dim_split_log=dsl)
+            torch.cuda.synchronize()
+            gpu_s.append(time.perf_counter() - t0)
+            assert g.built_on_device
+            del g
+        t0 = time.perf_counter()
+        h = C.HostTree(pts, nrm, a, lo, hi, dim_split_log=dsl)
+        t1 = time.perf_counter()
+        g = C.GpuTree(h)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        res[f"octree{dsl}"] = {"gpu_build_s": statistics.median(gpu_s), "host_build_s": t1 - t0,
+                               "upload_s": t2 - t1, "nodes": g.info.num_nodes}
+    ref = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        if O.ref_available():
+            t0 = time.perf_counter()
+            O.RefTree(pts, nrm, a, lo, hi, dim_split_log=2)
+            ref = time.perf_counter() - t0
+    v = res["octree2"]
+    return {
+        "metric": "tree build points/s", "value": (1 << 20) / v["gpu_build_s"],
+        "unit": "points/s", "n_gpus": 1, "steps": max(3, args.steps // 4), "warmup": 1,
+        "ms_per_step": v["gpu_build_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": "tree build: 1,048,576 torus points, leaf size 1; wall clock "
+                               "from host arrays to a device-resident tree"},
+        "tree_build": res,
+        "cpu_baseline": None if ref is None else {
+            "value": (1 << 20) / ref, "unit": "points/s", "cores": 1, "kind": "reference",
+            "sample": "the reference's Octree2 constructor on the same 1,048,576 points "
+                      "(single-threaded, as the reference builds)"},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -974,7 +1032,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload",
-                    choices=sorted(WORKLOADS) + ["serving", "batching", "differentiation"],
+                    choices=sorted(WORKLOADS) + ["serving", "batching", "differentiation",
+                                                 "tree_build"],
                     default="sbh_wn")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
@@ -988,7 +1047,7 @@ def main():
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     systems = {"serving": run_serving, "batching": run_batching,
-               "differentiation": run_differentiation}
+               "differentiation": run_differentiation, "tree_build": run_tree_build}
     if args.workload in systems and args.impl == "ours":
         print(json.dumps(systems[args.workload](args)), flush=True)
         return

@@ -142,6 +142,25 @@ int sbh_host_tree_load(const char* path, sbh_host_tree** out);
  * PyQuadtreeGPU/PyOctreeGPU's constructor (include/py_tree_gpu.h:38-49, 69-80).
  * The GPU tree does not reference the host tree after this returns. */
 int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_tree** out);
+/* Builds the tree on the device from host arrays (as sbh_host_tree_create
+ * takes them) and keeps it there: the same tree and device image as
+ * sbh_host_tree_create + sbh_gpu_tree_create, bit for bit.  No counterpart in
+ * the reference (its build is host-only, include/tree3d.h:338-371).  Leaf size
+ * 1 builds on the GPU; a leaf size above 1, or points the depth cap leaves
+ * sharing a leaf, need std::partition's order inside the leaf and are built on
+ * the host and uploaded.  *on_device (optional) tells which happened. */
+int sbh_gpu_tree_build(int dim, int dim_split_log, int leaf_size, int max_depth,
+                       const float* points, const float* normals, const float* masses, int64_t n,
+                       const float* min_corner, const float* max_corner, float alpha, int device,
+                       sbh_gpu_tree** out, int32_t* on_device);
+/* Copies the tree's device image out (any pointer may be NULL): points
+ * [n][4] (x, y, z, mass) and normals [n][4]; per node: centroid + diameter
+ * [nn][4], aggregate mass + normal [nn][4], topology [nn][4] (first child,
+ * children, start, end), AABB corners [nn][4] each, child masks
+ * [nn][max(1, branching/64)]; path codes [n]. */
+int sbh_gpu_tree_export(const sbh_gpu_tree* tree, float* pt_pm, float* pt_nrm, float* nd_cm,
+                        float* nd_agg, int32_t* nd_topo, float* nd_bmin, float* nd_bmax,
+                        uint64_t* nd_mask, uint64_t* pt_code);
 void sbh_gpu_tree_destroy(sbh_gpu_tree* tree);
 int sbh_gpu_tree_info(const sbh_gpu_tree* tree, sbh_tree_info* info);
 

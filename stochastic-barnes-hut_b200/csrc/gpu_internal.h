@@ -26,6 +26,50 @@ struct sbh_gpu_tree {
 
 namespace sbh {
 
+// Byte offsets of a tree's arrays inside its single device allocation
+// (256-byte aligned sub-arrays; see DevTree for the contents).
+struct TreeLayout {
+  size_t status, pm, nrm, cm, agg, topo, bmin, bmax, mask, code, bytes;
+};
+
+inline TreeLayout tree_layout(int64_t n, int64_t nn, int mw) {
+  TreeLayout L = {};
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    const size_t o = off;
+    off += ((b > 0 ? b : 1) + 255) & ~size_t(255);
+    return o;
+  };
+  L.status = take(sizeof(int));
+  L.pm = take(n * sizeof(float4));
+  L.nrm = take(n * sizeof(float4));
+  L.cm = take(nn * sizeof(float4));
+  L.agg = take(nn * sizeof(float4));
+  L.topo = take(nn * sizeof(int4));
+  L.bmin = take(nn * sizeof(float4));
+  L.bmax = take(nn * sizeof(float4));
+  L.mask = take((size_t)nn * mw * sizeof(uint64_t));
+  L.code = take(n * sizeof(uint64_t));
+  L.bytes = off;
+  return L;
+}
+
+// Points the tree's device image at the arrays of allocation `g->mem`.
+inline void bind_tree(sbh_gpu_tree* g, const TreeLayout& L) {
+  char* base = static_cast<char*>(g->mem);
+  g->d_status = reinterpret_cast<int*>(base + L.status);
+  DevTree& t = g->dev;
+  t.pt_pm = reinterpret_cast<const float4*>(base + L.pm);
+  t.pt_nrm = reinterpret_cast<const float4*>(base + L.nrm);
+  t.nd_cm = reinterpret_cast<const float4*>(base + L.cm);
+  t.nd_agg = reinterpret_cast<const float4*>(base + L.agg);
+  t.nd_topo = reinterpret_cast<const int4*>(base + L.topo);
+  t.nd_bmin = reinterpret_cast<const float4*>(base + L.bmin);
+  t.nd_bmax = reinterpret_cast<const float4*>(base + L.bmax);
+  t.nd_mask = reinterpret_cast<const unsigned long long*>(base + L.mask);
+  t.pt_code = reinterpret_cast<const unsigned long long*>(base + L.code);
+}
+
 // Makes `dev` current for the scope and restores the previous device.
 struct DeviceGuard {
   int prev = -1;

@@ -265,29 +265,17 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
                            (int)h.start[v], (int)h.end[v]);
   }
 
-  size_t off = 0;
-  auto take = [&](size_t b) {
-    size_t o = off;
-    off += align256(b > 0 ? b : 1);
-    return o;
-  };
-  const size_t o_status = take(sizeof(int));
-  const size_t o_pm = take(n * sizeof(float4)), o_nrm = take(n * sizeof(float4));
-  const size_t o_cm = take(nn * sizeof(float4)), o_agg = take(nn * sizeof(float4));
-  const size_t o_topo = take(nn * sizeof(int4));
-  const size_t o_bmin = take(nn * sizeof(float4)), o_bmax = take(nn * sizeof(float4));
-  const size_t o_mask = take((size_t)nn * mw * sizeof(uint64_t));
+  const sbh::TreeLayout L = sbh::tree_layout(n, nn, mw);
   std::vector<uint64_t> pt_code;
   int code_bits = 0, code_levels = 0;
   sbh::compute_path_codes(h, pt_code, &code_bits, &code_levels);
-  const size_t o_code = take(n * sizeof(uint64_t));
 
   sbh_gpu_tree* g = new (std::nothrow) sbh_gpu_tree();
   if (!g) return sbh::fail(SBH_ERR_OUT_OF_MEMORY, "host allocation failed");
   g->device = device;
   g->sm_count = prop.multiProcessorCount;
-  g->bytes = off;
-  cudaError_t e = cudaMalloc(&g->mem, off);
+  g->bytes = L.bytes;
+  cudaError_t e = cudaMalloc(&g->mem, L.bytes);
   if (e != cudaSuccess) {
     delete g;
     return cuda_fail(e, "cudaMalloc(tree)");
@@ -297,16 +285,16 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
     size_t off;
     const void* src;
     size_t bytes;
-  } copies[] = {{o_pm, pt_pm.data(), n * sizeof(float4)},
-                {o_nrm, pt_nrm.data(), n * sizeof(float4)},
-                {o_cm, nd_cm.data(), nn * sizeof(float4)},
-                {o_agg, nd_agg.data(), nn * sizeof(float4)},
-                {o_topo, nd_topo.data(), nn * sizeof(int4)},
-                {o_bmin, nd_bmin.data(), nn * sizeof(float4)},
-                {o_bmax, nd_bmax.data(), nn * sizeof(float4)},
-                {o_mask, h.mask.data(), (size_t)nn * mw * sizeof(uint64_t)},
-                {o_code, pt_code.data(), n * sizeof(uint64_t)}};
-  e = cudaMemset(base + o_status, 0, sizeof(int));
+  } copies[] = {{L.pm, pt_pm.data(), n * sizeof(float4)},
+                {L.nrm, pt_nrm.data(), n * sizeof(float4)},
+                {L.cm, nd_cm.data(), nn * sizeof(float4)},
+                {L.agg, nd_agg.data(), nn * sizeof(float4)},
+                {L.topo, nd_topo.data(), nn * sizeof(int4)},
+                {L.bmin, nd_bmin.data(), nn * sizeof(float4)},
+                {L.bmax, nd_bmax.data(), nn * sizeof(float4)},
+                {L.mask, h.mask.data(), (size_t)nn * mw * sizeof(uint64_t)},
+                {L.code, pt_code.data(), n * sizeof(uint64_t)}};
+  e = cudaMemset(base + L.status, 0, sizeof(int));
   for (const Copy& c : copies)
     if (e == cudaSuccess && c.bytes) e = cudaMemcpy(base + c.off, c.src, c.bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaEventCreate(&g->ev0);
@@ -317,17 +305,8 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
     delete g;
     return cuda_fail(e, "tree upload");
   }
-  g->d_status = reinterpret_cast<int*>(base + o_status);
+  sbh::bind_tree(g, L);
   sbh::DevTree& t = g->dev;
-  t.pt_pm = reinterpret_cast<const float4*>(base + o_pm);
-  t.pt_nrm = reinterpret_cast<const float4*>(base + o_nrm);
-  t.nd_cm = reinterpret_cast<const float4*>(base + o_cm);
-  t.nd_agg = reinterpret_cast<const float4*>(base + o_agg);
-  t.nd_topo = reinterpret_cast<const int4*>(base + o_topo);
-  t.nd_bmin = reinterpret_cast<const float4*>(base + o_bmin);
-  t.nd_bmax = reinterpret_cast<const float4*>(base + o_bmax);
-  t.nd_mask = reinterpret_cast<const unsigned long long*>(base + o_mask);
-  t.pt_code = reinterpret_cast<const unsigned long long*>(base + o_code);
   t.code_bits = code_bits;
   t.code_levels = code_levels;
   t.n = n;
@@ -345,7 +324,7 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
     g->box_hi[k] = h.bmax[k];
   }
   sbh::fill_info(h, &g->info);
-  g->info.device_bytes = off;
+  g->info.device_bytes = L.bytes;
   *out = g;
   return sbh::ok();
 }

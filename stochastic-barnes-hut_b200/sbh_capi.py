@@ -64,6 +64,10 @@ _SIGNATURES = {
     "sbh_eval_grad": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _P]),
     "sbh_eval_grad_device": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P]),
     "sbh_measure_pipe_rates": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P]),
+    "sbh_gpu_tree_build": (ctypes.c_int, [ctypes.c_int] * 4 + [_P, _P, _P, _I64, _P, _P,
+                                                               ctypes.c_float, ctypes.c_int, _P,
+                                                               _P]),
+    "sbh_gpu_tree_export": (ctypes.c_int, [_P] * 10),
     "sbh_host_tree_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "sbh_host_tree_load": (ctypes.c_int, [ctypes.c_char_p, _P]),
     "sbh_batch_tuning_init": (None, [_P]),
@@ -244,12 +248,53 @@ class GpuTree:
     def __init__(self, host: HostTree, device: int = 0):
         h = ctypes.c_void_p()
         _check(lib().sbh_gpu_tree_create(host.handle, device, ctypes.byref(h)))
+        self._adopt(h, device)
+        self.built_on_device = False
+
+    def _adopt(self, h, device):
         self.handle = h
         i = TreeInfo()
         _check(lib().sbh_gpu_tree_info(h, ctypes.byref(i)))
         self.info = i
         self.dim = i.dim
         self.device = device
+
+    @classmethod
+    def build(cls, points, normals, masses, min_corner, max_corner, alpha=1.0, dim_split_log=1,
+              leaf_size=1, max_depth=100, device: int = 0) -> "GpuTree":
+        """sbh_gpu_tree_build: the same tree as GpuTree(HostTree(...)), built on
+        the device (leaf size 1) or on the host (otherwise); `built_on_device`
+        tells which."""
+        pts = np.ascontiguousarray(points, np.float32)
+        n, dim = pts.shape
+        nrm = np.ascontiguousarray(normals, np.float32).reshape(n, dim)
+        m = np.ascontiguousarray(masses, np.float32).reshape(n)
+        lo = np.ascontiguousarray(min_corner, np.float32).reshape(dim)
+        hi = np.ascontiguousarray(max_corner, np.float32).reshape(dim)
+        h = ctypes.c_void_p()
+        on = ctypes.c_int32(0)
+        _check(lib().sbh_gpu_tree_build(dim, dim_split_log, leaf_size, max_depth, _ptr(pts),
+                                        _ptr(nrm), _ptr(m), n, _ptr(lo), _ptr(hi),
+                                        ctypes.c_float(alpha), device, ctypes.byref(h),
+                                        ctypes.byref(on)))
+        t = cls.__new__(cls)
+        t._adopt(h, device)
+        t.built_on_device = bool(on.value)
+        return t
+
+    def export(self) -> dict:
+        """sbh_gpu_tree_export: the device image as numpy arrays."""
+        n, nn = self.info.num_points, self.info.num_nodes
+        mw = max(1, (1 << (self.dim * self.info.dim_split_log)) >> 6)
+        out = dict(pt_pm=np.zeros((n, 4), np.float32), pt_nrm=np.zeros((n, 4), np.float32),
+                   nd_cm=np.zeros((nn, 4), np.float32), nd_agg=np.zeros((nn, 4), np.float32),
+                   nd_topo=np.zeros((nn, 4), np.int32), nd_bmin=np.zeros((nn, 4), np.float32),
+                   nd_bmax=np.zeros((nn, 4), np.float32), nd_mask=np.zeros((nn, mw), np.uint64),
+                   pt_code=np.zeros(n, np.uint64))
+        keys = ["pt_pm", "pt_nrm", "nd_cm", "nd_agg", "nd_topo", "nd_bmin", "nd_bmax", "nd_mask",
+                "pt_code"]
+        _check(lib().sbh_gpu_tree_export(self.handle, *[_ptr(out[k]) for k in keys]))
+        return out
 
     def eval(self, queries, p: Params, stream: int = 0, contribs: bool = False):
         """Blocking evaluation of host queries (n, dim): returns (values, kernel_ms[, counts])."""
