@@ -598,10 +598,11 @@ def serving_setup(C, seed=77, n_trees=32, n_requests=1500):
             pts, nrm, m = (W.gaussian_mixture(n, seed + i, dim=2) if kind == "gauss" else
                            W.circle_points(n, seed + i))
         lo, hi = W.padded_box(pts)
-        h1 = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=1)
-        h2 = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=2)
-        trees.append(dict(dim=dim, kind=kind, n=n, lo=lo, hi=hi, bh=h1, sbh=h2,
-                          root2=h2.info().root_children))
+        # built on the device (sbh_gpu_tree_build; the same trees as a host build)
+        g1 = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=1)
+        g2 = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=2)
+        trees.append(dict(dim=dim, kind=kind, n=n, lo=lo, hi=hi, bh=g1, sbh=g2,
+                          root2=g2.info.root_children))
     reqs = []
     for r in range(n_requests):
         ti = int(rng.integers(n_trees))
@@ -707,14 +708,11 @@ def serving_tuning(C, W, trees, reqs, gpus, n=256):
     batch: the first `n` requests of the stream, each once as stochastic BH and
     once as Barnes-Hut (untimed)."""
     import torch
-    gpus2 = {}
     entries, keep = [], []
     for r in reqs[:n]:
         t = trees[r["tree"]]
-        if r["tree"] not in gpus2:
-            gpus2[r["tree"]] = C.GpuTree(t["sbh"])
         dq = torch.from_numpy(np.ascontiguousarray(r["q"].T)).cuda()
-        for method, g in (("sbh", gpus2[r["tree"]]), ("bh", gpus[r["tree"]])):
+        for method, g in (("sbh", t["sbh"]), ("bh", t["bh"])):
             out = torch.empty(r["nq"], dtype=torch.float32, device="cuda")
             entries.append((g, serving_params(C, W, t, r, method), dq.data_ptr(), r["nq"],
                             out.data_ptr(), 0, 0))
@@ -731,7 +729,7 @@ def run_serving(args):
     import sbh_workloads as W
     t_setup = time.perf_counter()
     trees, reqs = serving_setup(C)
-    gpus = {i: C.GpuTree(t["bh"]) for i, t in enumerate(trees)}
+    gpus = {i: t["bh"] for i, t in enumerate(trees)}
     tuning, tune_info = serving_tuning(C, W, trees, reqs, gpus)
     server = C.Server(slots=3, slot_queries=1 << 20, max_requests_per_batch=4096, tuning=tuning)
     ids = {}

@@ -272,8 +272,11 @@ typedef struct sbh_server_stats {
 
 void sbh_server_config_init(sbh_server_config* cfg);
 int sbh_server_create(const sbh_server_config* cfg, sbh_server** out);
-/* Uploads a host tree and keeps it resident; *tree_id names it in requests. */
+/* Uploads a host tree and keeps it resident; *tree_id names it in requests.
+ * sbh_server_add_gpu_tree copies a device tree of the server's device (for
+ * instance one from sbh_gpu_tree_build); the caller keeps its own. */
 int sbh_server_add_tree(sbh_server* server, const sbh_host_tree* host, int32_t* tree_id);
+int sbh_server_add_gpu_tree(sbh_server* server, const sbh_gpu_tree* tree, int32_t* tree_id);
 /* Queues a request.  queries: host [dim][nq] float32; results: host [nq];
  * contribs: optional host [nq].  The buffers must stay valid until
  * sbh_server_wait reports the request finished. */

@@ -70,6 +70,9 @@ inline void bind_tree(sbh_gpu_tree* g, const TreeLayout& L) {
   t.pt_code = reinterpret_cast<const unsigned long long*>(base + L.code);
 }
 
+// A copy of a device tree (its own allocation and status word), on its device.
+int clone_gpu_tree(const sbh_gpu_tree* src, sbh_gpu_tree** out);
+
 // Makes `dev` current for the scope and restores the previous device.
 struct DeviceGuard {
   int prev = -1;

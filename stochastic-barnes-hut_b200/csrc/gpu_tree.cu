@@ -329,6 +329,36 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
   return sbh::ok();
 }
 
+int sbh::clone_gpu_tree(const sbh_gpu_tree* src, sbh_gpu_tree** out) {
+  *out = nullptr;
+  DeviceGuard guard(src->device);
+  sbh_gpu_tree* g = new (std::nothrow) sbh_gpu_tree();
+  if (!g) return sbh::fail(SBH_ERR_OUT_OF_MEMORY, "host allocation failed");
+  g->device = src->device;
+  g->sm_count = src->sm_count;
+  g->bytes = src->bytes;
+  g->info = src->info;
+  g->dev = src->dev;
+  for (int k = 0; k < 3; k++) {
+    g->box_lo[k] = src->box_lo[k];
+    g->box_hi[k] = src->box_hi[k];
+  }
+  cudaError_t e = cudaMalloc(&g->mem, src->bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(g->mem, src->mem, src->bytes, cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess) e = cudaEventCreate(&g->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&g->ev1);
+  if (e != cudaSuccess) {
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    cudaFree(g->mem);
+    delete g;
+    return cuda_fail(e, "tree copy");
+  }
+  sbh::bind_tree(g, sbh::tree_layout(src->dev.n, src->dev.nn, src->dev.mw));
+  cudaMemset(g->d_status, 0, sizeof(int));
+  *out = g;
+  return SBH_OK;
+}
+
 SBH_API void sbh_gpu_tree_destroy(sbh_gpu_tree* tree) {
   if (!tree) return;
   {

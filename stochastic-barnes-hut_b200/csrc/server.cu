@@ -661,11 +661,10 @@ SBH_API int sbh_server_create(const sbh_server_config* cfg_in, sbh_server** out)
   return sbh::ok();
 }
 
-SBH_API int sbh_server_add_tree(sbh_server* s, const sbh_host_tree* host, int32_t* tree_id) {
-  if (!s || !host || !tree_id) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null argument");
-  sbh_gpu_tree* g = nullptr;
-  int st = sbh_gpu_tree_create(host, s->cfg.device, &g);
-  if (st != SBH_OK) return st;
+namespace {
+
+// Registers a device tree the server now owns.
+int server_adopt(sbh_server* s, sbh_gpu_tree* g, int32_t* tree_id) {
   std::lock_guard<std::mutex> lock(s->mu);
   if ((int)s->trees.size() >= s->tree_cap) {
     sbh_gpu_tree_destroy(g);
@@ -681,6 +680,26 @@ SBH_API int sbh_server_add_tree(sbh_server* s, const sbh_host_tree* host, int32_
   s->h_trees.push_back(g->dev);
   *tree_id = id;
   return sbh::ok();
+}
+
+}  // namespace
+
+SBH_API int sbh_server_add_tree(sbh_server* s, const sbh_host_tree* host, int32_t* tree_id) {
+  if (!s || !host || !tree_id) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null argument");
+  sbh_gpu_tree* g = nullptr;
+  int st = sbh_gpu_tree_create(host, s->cfg.device, &g);
+  if (st != SBH_OK) return st;
+  return server_adopt(s, g, tree_id);
+}
+
+SBH_API int sbh_server_add_gpu_tree(sbh_server* s, const sbh_gpu_tree* tree, int32_t* tree_id) {
+  if (!s || !tree || !tree_id) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "null argument");
+  if (tree->device != s->cfg.device)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "the tree is on another device than the server");
+  sbh_gpu_tree* g = nullptr;
+  int st = sbh::clone_gpu_tree(tree, &g);
+  if (st != SBH_OK) return st;
+  return server_adopt(s, g, tree_id);
 }
 
 SBH_API int sbh_server_submit(sbh_server* s, int32_t tree_id, const sbh_params* p,

@@ -68,6 +68,7 @@ _SIGNATURES = {
                                                                ctypes.c_float, ctypes.c_int, _P,
                                                                _P]),
     "sbh_gpu_tree_export": (ctypes.c_int, [_P] * 10),
+    "sbh_server_add_gpu_tree": (ctypes.c_int, [_P, _P, _P]),
     "sbh_host_tree_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "sbh_host_tree_load": (ctypes.c_int, [ctypes.c_char_p, _P]),
     "sbh_batch_tuning_init": (None, [_P]),
@@ -476,10 +477,15 @@ class Server:
         self.handle = h
         self.dims = []
 
-    def add_tree(self, host: HostTree) -> int:
+    def add_tree(self, tree) -> int:
+        """A HostTree (uploaded) or a GpuTree of the server's device (copied)."""
         tid = ctypes.c_int32()
-        _check(lib().sbh_server_add_tree(self.handle, host.handle, ctypes.byref(tid)))
-        self.dims.append(host.info().dim)
+        if isinstance(tree, GpuTree):
+            _check(lib().sbh_server_add_gpu_tree(self.handle, tree.handle, ctypes.byref(tid)))
+            self.dims.append(tree.dim)
+        else:
+            _check(lib().sbh_server_add_tree(self.handle, tree.handle, ctypes.byref(tid)))
+            self.dims.append(tree.info().dim)
         return tid.value
 
     def submit(self, tree_id: int, queries, p: Params, contribs: bool = False) -> Request:

@@ -69,3 +69,16 @@ def test_gpu_build_falls_back_where_partition_order_matters():
     g = C.GpuTree.build(p, np.ones_like(p), np.ones(6, np.float32), -np.ones(3, np.float32),
                         np.ones(3, np.float32), max_depth=20)
     assert not g.built_on_device and g.info.depth == 20
+
+
+def test_server_serves_device_built_trees():
+    pts, nrm, a = W.torus_surface(30000, seed=8)
+    lo, hi = W.padded_box(pts)
+    g = C.GpuTree.build(pts, nrm, a, lo, hi, dim_split_log=2)
+    server = C.Server(slots=2, slot_queries=4096)
+    tid = server.add_tree(g)
+    q = W.uniform_queries(10000, seed=9)
+    p = C.params(method=C.STOCHASTIC, kernel=C.WINDING_NUMBER, samples_per_subdomain=2, seed=1)
+    r = server.submit(tid, q, p)
+    assert bits_equal(r.wait(), g.eval(q, p)[0])
+    server.close()
