@@ -1,6 +1,6 @@
 // Batched evaluation: a list of requests -- each its own tree, method, kernel,
-// parameters and query count -- runs as one fixed pipeline of four kernels,
-// captured once as a CUDA graph:
+// parameters and query count -- runs as one fixed pipeline, captured once as a
+// CUDA graph:
 //
 //   batch_keys_kernel     Morton bucket of every query of every request, inside
 //                         its tree's root box, with a per-request bucket count
@@ -9,12 +9,14 @@
 //                         request's buckets follow the previous request's, so
 //                         the scan also places every request at its offset);
 //   batch_scatter_kernel  the sorted position of every query;
-//   batch_eval_kernel     a persistent kernel: warps take work units (32 queries
-//                         of a Barnes-Hut or brute-force request, or a pair of
-//                         sampler queries) from an atomic counter and run the
-//                         same device routines as the single-call kernels
-//                         (tasks.cuh), dispatching on method, kernel and
-//                         dimension per unit.
+//   batch_eval_kernel<C>  three persistent kernels, one per method class
+//                         (Barnes-Hut, sampler, brute force), as parallel
+//                         branches of the graph: warps take that class's work
+//                         units from its atomic counter and run the same device
+//                         routines as the single-call kernels (tasks.cuh),
+//                         dispatching on kernel and dimension per unit.  Each
+//                         is compiled for its own method alone, so none carries
+//                         the registers or the call overhead of the others.
 //
 // Every launch parameter of the graph is fixed (grids are persistent; sizes and
 // the request table live in device memory, refreshed by one host-to-device copy
@@ -122,22 +124,28 @@ __global__ void batch_scatter_kernel(const BatchHeader* __restrict__ hdr,
 }
 
 constexpr int kTreeWords = (int)((sizeof(DevTree) + 15) / 16 * 4);
+constexpr int kItemWords = (int)((sizeof(BatchItem) + 15) / 16 * 4);
 
-// One work unit of each method, as separate functions so each is register
-// allocated on its own (the dispatcher below stays small).
-template <int DIM, int K, bool VOTE>
-__device__ __noinline__ void run_bh(const DevTree& t, const BatchItem& it, long long u,
-                                    const int* ord, float* scratch, int stack_cap, int* status) {
+// One work unit of a request, by method class; inlined into that class's
+// kernel.  `t` is a register copy of the request's tree record.
+template <int DIM, int K>
+__device__ __forceinline__ void run_bh(const DevTree& t, const BatchItem& it, long long u,
+                                       const int* ord, float* scratch, int stack_cap,
+                                       int* status) {
   const long long s0 = u * it.unit_queries;
   const long long s1 = min(it.nq, s0 + it.unit_queries);
-  bh_warp_task<DIM, K, VOTE>(t, it.q, it.nq, ord, s0, s1, it.beta, it.kp, it.out, it.contribs,
-                             status, reinterpret_cast<BhStackEntry*>(scratch), stack_cap,
-                             it.self_mass);
+  BhStackEntry* stk = reinterpret_cast<BhStackEntry*>(scratch);
+  if (it.method == 2)
+    bh_warp_task<DIM, K, true>(t, it.q, it.nq, ord, s0, s1, it.beta, it.kp, it.out, it.contribs,
+                               status, stk, stack_cap, it.self_mass);
+  else
+    bh_warp_task<DIM, K, false>(t, it.q, it.nq, ord, s0, s1, it.beta, it.kp, it.out,
+                                it.contribs, status, stk, stack_cap, it.self_mass);
 }
 
 template <int DIM, int K>
-__device__ __noinline__ void run_sbh(const DevTree& t, const BatchItem& it, long long u,
-                                     const int* ord, float* scratch, int* status) {
+__device__ __forceinline__ void run_sbh(const DevTree& t, const BatchItem& it, long long u,
+                                        const int* ord, float* scratch, int* status) {
   const int lane = threadIdx.x & 31;
   const SbhWarpSmem<float> ws = sbh_carve<float>(scratch, t.root_children);
   const long long s0 = u * it.unit_queries;
@@ -157,26 +165,43 @@ __device__ __noinline__ void run_sbh(const DevTree& t, const BatchItem& it, long
 }
 
 template <int DIM, int K>
-__device__ __noinline__ void run_bf(const DevTree& t, const BatchItem& it, long long u) {
+__device__ __forceinline__ void run_bf(const DevTree& t, const BatchItem& it, long long u) {
   const long long s0 = u * kUnitQueriesWarp;
   bf_warp_task<DIM, K>(t, it.q, it.nq, s0, min(it.nq, s0 + kUnitQueriesWarp), it.kp, it.out,
                        it.contribs, it.self_mass);
 }
 
-template <int DIM, int K>
+template <int CLASS, int DIM, int K>
 __device__ __forceinline__ void run_unit(const DevTree& t, const BatchItem& it, long long u,
                                          const int* order, float* scratch, int stack_cap,
                                          int* status) {
   const int* ord = it.sort_bits > 0 ? order + it.sort_base : nullptr;
-  switch (it.method) {
-    case 1: run_bh<DIM, K, false>(t, it, u, ord, scratch, stack_cap, status); break;
-    case 2: run_bh<DIM, K, true>(t, it, u, ord, scratch, stack_cap, status); break;
-    case 3: run_sbh<DIM, K>(t, it, u, ord, scratch, status); break;
-    default: run_bf<DIM, K>(t, it, u); break;
+  if (CLASS == kClassBh) run_bh<DIM, K>(t, it, u, ord, scratch, stack_cap, status);
+  if (CLASS == kClassSbh) run_sbh<DIM, K>(t, it, u, ord, scratch, status);
+  if (CLASS == kClassBf) run_bf<DIM, K>(t, it, u);
+}
+
+template <int CLASS>
+__device__ __forceinline__ void dispatch_unit(const DevTree& t, const BatchItem& it, long long u,
+                                              const int* order, float* scratch, int stack_cap,
+                                              int* status) {
+  const int key = (t.dim == 3 ? 0 : 4) + it.kernel;
+  switch (key) {
+    case 0: run_unit<CLASS, 3, kGravity>(t, it, u, order, scratch, stack_cap, status); break;
+    case 1: run_unit<CLASS, 3, kWindingNumber>(t, it, u, order, scratch, stack_cap, status); break;
+    case 2: run_unit<CLASS, 3, kSmoothDist>(t, it, u, order, scratch, stack_cap, status); break;
+    case 3: run_unit<CLASS, 3, kPlummer>(t, it, u, order, scratch, stack_cap, status); break;
+    case 4: run_unit<CLASS, 2, kGravity>(t, it, u, order, scratch, stack_cap, status); break;
+    case 5: run_unit<CLASS, 2, kWindingNumber>(t, it, u, order, scratch, stack_cap, status); break;
+    case 6: run_unit<CLASS, 2, kSmoothDist>(t, it, u, order, scratch, stack_cap, status); break;
+    default: run_unit<CLASS, 2, kPlummer>(t, it, u, order, scratch, stack_cap, status); break;
   }
 }
 
-__global__ void __launch_bounds__(kEvalThreads, 8)
+// The persistent kernel of one method class: warps take that class's work
+// units from its counter and run them.
+template <int CLASS>
+__global__ void __launch_bounds__(kEvalThreads, CLASS == kClassSbh ? 8 : 1)
     batch_eval_kernel(BatchHeader* hdr, const BatchItem* __restrict__ items,
                       const DevTree* __restrict__ trees, const int* __restrict__ order,
                       int* status, int warp_words, int stack_cap) {
@@ -184,40 +209,68 @@ __global__ void __launch_bounds__(kEvalThreads, 8)
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   float* wbase = reinterpret_cast<float*>(s_eval) + (size_t)warp * warp_words;
-  DevTree& t = *reinterpret_cast<DevTree*>(wbase);
-  float* scratch = wbase + kTreeWords;
-  const int n = hdr->n_items;
-  const long long total = hdr->total_units;
-  int cached_tree = -1;
+  // Per-warp shared memory: the current tree record, the current request,
+  // then the class's scratch.  The walks read both records from there instead
+  // of holding them in registers.
+  const DevTree& ts = *reinterpret_cast<const DevTree*>(wbase);
+  const BatchItem& it = *reinterpret_cast<const BatchItem*>(wbase + kTreeWords);
+  float* scratch = wbase + kTreeWords + kItemWords;
+  const int ib = hdr->item_begin[CLASS], ie = hdr->item_end[CLASS];
+  const long long total = hdr->total_units[CLASS];
+  int cached_tree = -1, cached_item = -1;
   for (;;) {
     unsigned long long unit = 0;
-    if (lane == 0) unit = atomicAdd(&hdr->next_unit, 1ull);
+    if (lane == 0) unit = atomicAdd(&hdr->next_unit[CLASS], 1ull);
     unit = __shfl_sync(0xffffffffu, unit, 0);
     if ((long long)unit >= total) break;
-    const int item = find_item_by(items, n, (long long)unit, &BatchItem::unit_base);
-    const BatchItem& it = items[item];
-    if (it.tree != cached_tree) {
+    const int item = ib + find_item_by(items + ib, ie - ib, (long long)unit, &BatchItem::unit_base);
+    if (item != cached_item) {
       __syncwarp();
-      const int* src = reinterpret_cast<const int*>(trees + it.tree);
+      const int* src = reinterpret_cast<const int*>(items + item);
+      int* dst = reinterpret_cast<int*>(wbase + kTreeWords);
+      for (int w = lane; w < (int)(sizeof(BatchItem) / 4); w += 32) dst[w] = __ldg(src + w);
+      cached_item = item;
+      __syncwarp();
+    }
+    if (it.tree != cached_tree) {
+      const int tree = it.tree;
+      __syncwarp();
+      const int* src = reinterpret_cast<const int*>(trees + tree);
       int* dst = reinterpret_cast<int*>(wbase);
       for (int w = lane; w < (int)(sizeof(DevTree) / 4); w += 32) dst[w] = __ldg(src + w);
-      cached_tree = it.tree;
+      cached_tree = tree;
       __syncwarp();
     }
     const long long u = (long long)unit - it.unit_base;
-    const int key = (t.dim == 3 ? 0 : 4) + it.kernel;
-    switch (key) {
-      case 0: run_unit<3, kGravity>(t, it, u, order, scratch, stack_cap, status); break;
-      case 1: run_unit<3, kWindingNumber>(t, it, u, order, scratch, stack_cap, status); break;
-      case 2: run_unit<3, kSmoothDist>(t, it, u, order, scratch, stack_cap, status); break;
-      case 3: run_unit<3, kPlummer>(t, it, u, order, scratch, stack_cap, status); break;
-      case 4: run_unit<2, kGravity>(t, it, u, order, scratch, stack_cap, status); break;
-      case 5: run_unit<2, kWindingNumber>(t, it, u, order, scratch, stack_cap, status); break;
-      case 6: run_unit<2, kSmoothDist>(t, it, u, order, scratch, stack_cap, status); break;
-      default: run_unit<2, kPlummer>(t, it, u, order, scratch, stack_cap, status); break;
+    if constexpr (CLASS == kClassSbh) {
+      // The sampler keeps the record in shared memory: it needs its registers.
+      dispatch_unit<CLASS>(ts, it, u, order, scratch, stack_cap, status);
+    } else {
+      // The walks keep it in registers (no shared re-reads after each fence).
+      const DevTree t = ts;
+      dispatch_unit<CLASS>(t, it, u, order, scratch, stack_cap, status);
     }
     __syncwarp();
   }
+}
+
+// Per-warp shared words of a class's kernel: the tree record, then the class's
+// scratch (Barnes-Hut stack or sampler scratch).
+int class_warp_words(int cls, const BatchEngine::Limits& lim) {
+  int scratch = 0;
+  if (cls == kClassBh) scratch = (lim.max_tree_depth + 2) * (int)sizeof(BhStackEntry) / 4;
+  if (cls == kClassSbh) scratch = sbh_warp_words<float>(lim.max_root_children);
+  return kTreeWords + kItemWords + (scratch + 3) / 4 * 4;
+}
+
+template <int CLASS>
+void setup_class(size_t smem, int* per_sm) {
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(batch_eval_kernel<CLASS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_eval_kernel<CLASS>, kEvalThreads, smem);
+  *per_sm = std::max(1, n);
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -258,19 +311,12 @@ BatchEngine::BatchEngine(const Limits& lim, int sm_count) : lim_(lim), sm_count_
   d_hist_ = reinterpret_cast<unsigned*>(b + o_hist);
   d_order_ = reinterpret_cast<int*>(b + o_order);
   if (cudaMallocHost(&h_stage_, o_keys) != cudaSuccess) h_stage_ = nullptr;
-  // Per-warp shared memory: the tree record, then the larger of the
-  // Barnes-Hut stack and the sampler's scratch.
-  const int stack_words = (lim_.max_tree_depth + 2) * (int)sizeof(BhStackEntry) / 4;
-  const int scratch = std::max(stack_words, sbh_warp_words<float>(lim_.max_root_children));
-  const int warp_words = kTreeWords + (scratch + 3) / 4 * 4;
-  eval_smem_ = (size_t)kEvalWarps * warp_words * sizeof(float);
-  if (eval_smem_ > 48 * 1024)
-    cudaFuncSetAttribute(batch_eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)eval_smem_);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_eval_kernel, kEvalThreads,
-                                                eval_smem_);
-  per_sm_ = std::max(1, per_sm);
+  // Per-warp shared memory of each class's kernel.
+  for (int c = 0; c < kClasses; c++)
+    eval_smem_[c] = (size_t)kEvalWarps * class_warp_words(c, lim_) * sizeof(float);
+  setup_class<kClassBh>(eval_smem_[kClassBh], &per_sm_[kClassBh]);
+  setup_class<kClassSbh>(eval_smem_[kClassSbh], &per_sm_[kClassSbh]);
+  setup_class<kClassBf>(eval_smem_[kClassBf], &per_sm_[kClassBf]);
 }
 
 BatchEngine::~BatchEngine() {
@@ -289,7 +335,10 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
       tuning.bh_unit > 32)
     return "batch tuning out of range";
   if ((int)items.size() > lim_.max_items) return "too many requests in one batch";
-  long long sort_base = 0, bucket_base = 0, unit_base = 0;
+  std::stable_sort(items.begin(), items.end(), [](const BatchItem& a, const BatchItem& b) {
+    return batch_class(a.method) < batch_class(b.method);
+  });
+  long long sort_base = 0, bucket_base = 0, unit_base[kClasses] = {0, 0, 0};
   for (BatchItem& it : items) {
     if (it.tree < 0 || it.tree >= (int)host_trees.size()) return "request names an unknown tree";
     const DevTree& t = host_trees[it.tree];
@@ -302,7 +351,7 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
     it.sort_base = sort_base;
     it.bucket_base = bucket_base;
     it.buckets = it.sort_bits > 0 ? (1LL << (t.dim * it.sort_bits)) : 1;
-    it.unit_base = unit_base;
+    it.unit_base = unit_base[batch_class(it.method)];
     // Work unit: sampler queries per warp (tuned); Barnes-Hut queries per warp
     // walk (tuned; vote keeps 32, its acceptance is defined over 32 queries);
     // brute force 32 queries per warp.
@@ -312,42 +361,69 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
     it.units = (it.nq + it.unit_queries - 1) / it.unit_queries;
     sort_base += it.nq;
     bucket_base += it.buckets;
-    unit_base += it.units;
+    unit_base[batch_class(it.method)] += it.units;
   }
   if (sort_base > lim_.max_queries) return "batch exceeds the engine's query capacity";
   if (bucket_base > max_buckets(lim_)) return "batch exceeds the engine's bucket capacity";
   return "";
 }
 
-cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status, int blocks,
+cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status, int per_sm_cap,
                                  cudaGraphExec_t* out) {
   *out = nullptr;
-  // Captured on a private stream (the caller's may be the legacy default
+  // Captured on private streams (the caller's may be the legacy default
   // stream, which cannot be captured); the graph is launched on the caller's.
-  cudaStream_t stream = nullptr;
-  cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) return e;
+  // The query bucketing runs first, then the three class kernels as parallel
+  // branches of the graph: they share no state but the item table.
+  cudaStream_t st[1 + kClasses] = {};
+  cudaEvent_t ev[1 + kClasses] = {};
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i <= kClasses && e == cudaSuccess; i++) {
+    e = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+  }
   cudaGraph_t graph = nullptr;
-  e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(st[0], cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const int aux_blocks = sm_count_ * 4;
+    const int stack_cap = lim_.max_tree_depth + 2;
+    cudaMemsetAsync(d_hist_, 0, sizeof(unsigned) * max_buckets(lim_), st[0]);
+    batch_keys_kernel<<<aux_blocks, kAuxThreads, 0, st[0]>>>(d_header_, d_items_, d_keys_,
+                                                             d_hist_);
+    batch_scan_kernel<<<1, kScanThreads, 0, st[0]>>>(d_header_, d_hist_);
+    batch_scatter_kernel<<<aux_blocks, kAuxThreads, 0, st[0]>>>(d_header_, d_items_, d_keys_,
+                                                                d_hist_, d_order_);
+    cudaEventRecord(ev[0], st[0]);
+    for (int c = 0; c < kClasses; c++) {
+      cudaStream_t s = c == 0 ? st[0] : st[c];
+      if (c > 0) cudaStreamWaitEvent(s, ev[0], 0);
+      const int per_sm = per_sm_cap > 0 ? std::min(per_sm_cap, per_sm_[c]) : per_sm_[c];
+      const int blocks = per_sm * sm_count_;
+      const int words = class_warp_words(c, lim_);
+      if (c == kClassBh)
+        batch_eval_kernel<kClassBh><<<blocks, kEvalThreads, eval_smem_[c], s>>>(
+            d_header_, d_items_, d_trees, d_order_, d_status, words, stack_cap);
+      else if (c == kClassSbh)
+        batch_eval_kernel<kClassSbh><<<blocks, kEvalThreads, eval_smem_[c], s>>>(
+            d_header_, d_items_, d_trees, d_order_, d_status, words, stack_cap);
+      else
+        batch_eval_kernel<kClassBf><<<blocks, kEvalThreads, eval_smem_[c], s>>>(
+            d_header_, d_items_, d_trees, d_order_, d_status, words, stack_cap);
+      if (c > 0) {
+        cudaEventRecord(ev[c], s);
+        cudaStreamWaitEvent(st[0], ev[c], 0);
+      }
+    }
+    e = cudaStreamEndCapture(st[0], &graph);
+  }
+  for (int i = 0; i <= kClasses; i++) {
+    if (ev[i]) cudaEventDestroy(ev[i]);
+    if (st[i]) cudaStreamDestroy(st[i]);
+  }
   if (e != cudaSuccess) {
-    cudaStreamDestroy(stream);
+    if (graph) cudaGraphDestroy(graph);
     return e;
   }
-  const int aux_blocks = sm_count_ * 4;
-  const int stack_cap = lim_.max_tree_depth + 2;
-  const int stack_words = stack_cap * (int)sizeof(BhStackEntry) / 4;
-  const int scratch = std::max(stack_words, sbh_warp_words<float>(lim_.max_root_children));
-  const int warp_words = kTreeWords + (scratch + 3) / 4 * 4;
-  cudaMemsetAsync(d_hist_, 0, sizeof(unsigned) * max_buckets(lim_), stream);
-  batch_keys_kernel<<<aux_blocks, kAuxThreads, 0, stream>>>(d_header_, d_items_, d_keys_, d_hist_);
-  batch_scan_kernel<<<1, kScanThreads, 0, stream>>>(d_header_, d_hist_);
-  batch_scatter_kernel<<<aux_blocks, kAuxThreads, 0, stream>>>(d_header_, d_items_, d_keys_,
-                                                              d_hist_, d_order_);
-  batch_eval_kernel<<<blocks, kEvalThreads, eval_smem_, stream>>>(
-      d_header_, d_items_, d_trees, d_order_, d_status, warp_words, stack_cap);
-  e = cudaStreamEndCapture(stream, &graph);
-  cudaStreamDestroy(stream);
-  if (e != cudaSuccess) return e;
   e = cudaGraphInstantiate(out, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) *out = nullptr;
@@ -364,24 +440,31 @@ cudaError_t BatchEngine::launch(const std::vector<BatchItem>& items, const DevTr
     captured_trees_ = d_trees;
     captured_status_ = d_status;
   }
-  const int per_sm = tuning.blocks_per_sm > 0 ? std::min(tuning.blocks_per_sm, per_sm_) : per_sm_;
-  const int blocks = per_sm * sm_count_;
+  const int cap = std::max(0, tuning.blocks_per_sm);
   cudaGraphExec_t exec = nullptr;
   for (const Graph& g : graphs_)
-    if (g.blocks == blocks) exec = g.exec;
+    if (g.blocks == cap) exec = g.exec;
   if (!exec) {
-    cudaError_t e = capture(d_trees, d_status, blocks, &exec);
+    cudaError_t e = capture(d_trees, d_status, cap, &exec);
     if (e != cudaSuccess) return e;
-    graphs_.push_back(Graph{blocks, exec});
+    graphs_.push_back(Graph{cap, exec});
   }
   BatchHeader h = {};
   h.n_items = (int)items.size();
-  for (const BatchItem& it : items) {
+  for (int c = 0; c < kClasses; c++) h.item_begin[c] = h.item_end[c] = 0;
+  int prev = -1;
+  for (int i = 0; i < (int)items.size(); i++) {
+    const BatchItem& it = items[i];
+    const int c = batch_class(it.method);
+    if (c != prev) {
+      h.item_begin[c] = i;
+      prev = c;
+    }
+    h.item_end[c] = i + 1;
     h.total_queries += it.nq;
     h.total_buckets += it.buckets;
-    h.total_units += it.units;
+    h.total_units[c] += it.units;
   }
-  h.next_unit = 0;
   char* st = static_cast<char*>(h_stage_);
   std::memcpy(st, &h, sizeof(h));
   const size_t o_items = align256(sizeof(BatchHeader));

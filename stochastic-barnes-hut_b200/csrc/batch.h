@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -34,18 +35,27 @@ struct BatchItem {
   long long sort_base;       // first position of this request in the batch order array
   long long bucket_base;     // first bucket of this request
   long long buckets;         // buckets of this request
-  long long unit_base;       // first work unit of this request
+  long long unit_base;       // first work unit of this request within its class
   long long units;           // work units of this request
   float box_lo[3], box_hi[3];  // Morton box (the tree's root AABB)
 };
+
+// Requests are evaluated by one persistent kernel per method class (each
+// compiled for its own method, so none pays for the others' registers):
+enum BatchClass : int { kClassBh = 0, kClassSbh = 1, kClassBf = 2, kClasses = 3 };
+
+__host__ __device__ inline int batch_class(int method) {
+  return method == 3 ? kClassSbh : (method == 1 || method == 2) ? kClassBh : kClassBf;
+}
 
 struct BatchHeader {
   int n_items;
   int pad;
   long long total_queries;
   long long total_buckets;
-  long long total_units;
-  unsigned long long next_unit;  // work counter of the persistent kernel
+  int item_begin[kClasses], item_end[kClasses];  // each class's items are contiguous
+  long long total_units[kClasses];
+  unsigned long long next_unit[kClasses];  // work counters of the persistent kernels
 };
 
 // Queries per work unit (one warp task) of brute force: 32, a lane each.  The
@@ -77,8 +87,9 @@ class BatchEngine {
   BatchEngine(const BatchEngine&) = delete;
   BatchEngine& operator=(const BatchEngine&) = delete;
 
-  // Fills item bookkeeping (sort/bucket/unit ranges, sort bits) for `items`
-  // in place and checks limits.  Returns an error string or "".
+  // Orders `items` by method class (stably) and fills their bookkeeping
+  // (sort/bucket/unit ranges, sort bits) in place; checks limits.  Returns an
+  // error string or "".
   std::string plan(std::vector<BatchItem>& items, const std::vector<DevTree>& host_trees,
                    const Tuning& tuning) const;
   // Enqueues the batch on `stream` (items already planned with `tuning`):
@@ -89,20 +100,23 @@ class BatchEngine {
 
   const Limits& limits() const { return lim_; }
   size_t device_bytes() const { return dev_bytes_; }
-  // CTAs per SM of the evaluation kernel at full occupancy.
-  int max_blocks_per_sm() const { return per_sm_; }
+  // CTAs per SM of the evaluation kernels at full occupancy (the largest).
+  int max_blocks_per_sm() const {
+    return std::max(per_sm_[0], std::max(per_sm_[1], per_sm_[2]));
+  }
 
  private:
   struct Graph {
-    int blocks = 0;
+    int blocks = 0;  // the tuning's CTAs-per-SM cap (0: none)
     cudaGraphExec_t exec = nullptr;
   };
-  cudaError_t capture(const DevTree* d_trees, int* d_status, int blocks, cudaGraphExec_t* out);
+  cudaError_t capture(const DevTree* d_trees, int* d_status, int per_sm_cap,
+                      cudaGraphExec_t* out);
 
   Limits lim_;
   int sm_count_;
-  int per_sm_ = 1;
-  size_t eval_smem_ = 0;
+  int per_sm_[kClasses] = {1, 1, 1};
+  size_t eval_smem_[kClasses] = {0, 0, 0};
   // device buffers
   void* dev_ = nullptr;
   size_t dev_bytes_ = 0;
@@ -113,7 +127,7 @@ class BatchEngine {
   int* d_order_ = nullptr;
   // pinned staging of header + items
   void* h_stage_ = nullptr;
-  // captured pipelines, one per evaluation grid size
+  // captured pipelines, one per CTAs-per-SM cap
   std::vector<Graph> graphs_;
   const DevTree* captured_trees_ = nullptr;
   int* captured_status_ = nullptr;
