@@ -2,9 +2,11 @@
 // parameters and query count -- runs as one fixed pipeline, captured once as a
 // CUDA graph:
 //
+//   batch_bbox_kernel     the bounding box of every request's queries;
 //   batch_keys_kernel     Morton bucket of every query of every request, inside
-//                         its tree's root box, with a per-request bucket count
-//                         sized to the request (about 8 queries per bucket);
+//                         its request's query box, with a per-request bucket
+//                         count sized to the request (about 8 queries per
+//                         bucket);
 //   batch_scan_kernel     one exclusive scan over all requests' buckets (each
 //                         request's buckets follow the previous request's, so
 //                         the scan also places every request at its offset);
@@ -53,24 +55,92 @@ __device__ __forceinline__ unsigned spread(unsigned v, int bits, int stride) {
   return r;
 }
 
+// Order-preserving map of floats to unsigned ints (for atomicMax), and back.
+__device__ __forceinline__ unsigned to_ordered(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float from_ordered(unsigned u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// Per request, the bounding box of its queries (NaN queries excluded):
+// qbox[6 * item + d] = ~to_ordered(min_d) and qbox[6 * item + 3 + d] =
+// to_ordered(max_d), both reduced with atomicMax from zero.  A warp takes 32
+// consecutive queries; while they all belong to one request it reduces them
+// in registers and flushes once per request it met.
+__global__ void batch_bbox_kernel(const BatchHeader* __restrict__ hdr,
+                                  const BatchItem* __restrict__ items, unsigned* qbox) {
+  const int n = hdr->n_items;
+  const long long total = hdr->total_queries;
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * blockDim.x / 32;
+  const long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  int cur = -1;
+  unsigned acc[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+  auto flush = [&]() {
+    if (cur >= 0 && lane == 0)
+      for (int k = 0; k < 6; k++)
+        if (acc[k]) atomicMax(qbox + 6 * (size_t)cur + k, acc[k]);
+  };
+  for (long long base = wid * 32; base < total; base += warps * 32) {
+    const long long g = base + lane;
+    int item = -1;
+    unsigned v[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+    if (g < total) {
+      item = find_item_by(items, n, g, &BatchItem::sort_base);
+      const BatchItem& it = items[item];
+      if (it.sort_bits > 0) {
+        const long long i = g - it.sort_base;
+        for (int d = 0; d < it.dim; d++) {
+          const float x = it.q[d * it.nq + i];
+          if (x == x) {
+            v[d] = ~to_ordered(x);
+            v[3 + d] = to_ordered(x);
+          }
+        }
+      }
+    }
+    const int first = __shfl_sync(0xffffffffu, item, 0);
+    if (__all_sync(0xffffffffu, item == first)) {
+      if (first != cur) {
+        flush();
+        cur = first;
+        for (int k = 0; k < 6; k++) acc[k] = 0u;
+      }
+      for (int k = 0; k < 6; k++) acc[k] = max(acc[k], __reduce_max_sync(0xffffffffu, v[k]));
+    } else if (item >= 0) {
+      for (int k = 0; k < 6; k++)
+        if (v[k]) atomicMax(qbox + 6 * (size_t)item + k, v[k]);
+    }
+  }
+  flush();
+}
+
+// Morton bucket of every query inside its request's query box (as the
+// single-call sort does), counted into the request's buckets.
 __global__ void batch_keys_kernel(const BatchHeader* __restrict__ hdr,
-                                  const BatchItem* __restrict__ items, unsigned* keys,
+                                  const BatchItem* __restrict__ items,
+                                  const unsigned* __restrict__ qbox, unsigned* keys,
                                   unsigned* hist) {
   const int n = hdr->n_items;
   const long long total = hdr->total_queries;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
        g += (long long)gridDim.x * blockDim.x) {
-    const BatchItem& it = items[find_item_by(items, n, g, &BatchItem::sort_base)];
+    const int item = find_item_by(items, n, g, &BatchItem::sort_base);
+    const BatchItem& it = items[item];
     const long long i = g - it.sort_base;
     unsigned key = 0;
     const int bits = it.sort_bits;
     if (bits > 0) {
       const float cells = (float)(1 << bits);
       const int dim = it.dim;
+      const unsigned* box = qbox + 6 * (size_t)item;
       unsigned c[3] = {0u, 0u, 0u};
       for (int d = 0; d < dim; d++) {
-        const float ext = it.box_hi[d] - it.box_lo[d];
-        float f = ext > 0.f ? (it.q[d * it.nq + i] - it.box_lo[d]) * (cells / ext) : 0.f;
+        const float lo = from_ordered(~__ldg(box + d)), hi = from_ordered(__ldg(box + 3 + d));
+        const float ext = hi - lo;
+        float f = ext > 0.f ? (it.q[d * it.nq + i] - lo) * (cells / ext) : 0.f;
         f = f == f ? fminf(fmaxf(f, 0.f), cells - 1.f) : 0.f;
         c[d] = (unsigned)f;
       }
@@ -199,9 +269,12 @@ __device__ __forceinline__ void dispatch_unit(const DevTree& t, const BatchItem&
 }
 
 // The persistent kernel of one method class: warps take that class's work
-// units from its counter and run them.
+// units from its counter and run them.  Minimum CTAs per SM: the single-call
+// kernels' occupancy (sampler 8 at 64 registers, Barnes-Hut 10 at 48).
 template <int CLASS>
-__global__ void __launch_bounds__(kEvalThreads, CLASS == kClassSbh ? 8 : 1)
+__global__ void __launch_bounds__(kEvalThreads, CLASS == kClassSbh  ? 8
+                                                : CLASS == kClassBh ? 10
+                                                                    : 1)
     batch_eval_kernel(BatchHeader* hdr, const BatchItem* __restrict__ items,
                       const DevTree* __restrict__ trees, const int* __restrict__ order,
                       int* status, int warp_words, int stack_cap) {
@@ -242,11 +315,12 @@ __global__ void __launch_bounds__(kEvalThreads, CLASS == kClassSbh ? 8 : 1)
       __syncwarp();
     }
     const long long u = (long long)unit - it.unit_base;
-    if constexpr (CLASS == kClassSbh) {
-      // The sampler keeps the record in shared memory: it needs its registers.
+    if constexpr (CLASS != kClassBf) {
+      // The traversals read the record from shared memory: a register copy
+      // costs them occupancy (Barnes-Hut) or spills (sampler).
       dispatch_unit<CLASS>(ts, it, u, order, scratch, stack_cap, status);
     } else {
-      // The walks keep it in registers (no shared re-reads after each fence).
+      // Brute force keeps it in registers.
       const DevTree t = ts;
       dispatch_unit<CLASS>(t, it, u, order, scratch, stack_cap, status);
     }
@@ -254,23 +328,51 @@ __global__ void __launch_bounds__(kEvalThreads, CLASS == kClassSbh ? 8 : 1)
   }
 }
 
-// Per-warp shared words of a class's kernel: the tree record, then the class's
-// scratch (Barnes-Hut stack or sampler scratch).
-int class_warp_words(int cls, const BatchEngine::Limits& lim) {
+// Per-warp shared words of a class's kernel for a launch shape: the tree and
+// request records, then the class's scratch (Barnes-Hut stack of `bh_stack`
+// entries, or sampler scratch for roots of up to `sbh_r` children).
+int class_warp_words(int cls, int bh_stack, int sbh_r) {
   int scratch = 0;
-  if (cls == kClassBh) scratch = (lim.max_tree_depth + 2) * (int)sizeof(BhStackEntry) / 4;
-  if (cls == kClassSbh) scratch = sbh_warp_words<float>(lim.max_root_children);
+  if (cls == kClassBh) scratch = bh_stack * (int)sizeof(BhStackEntry) / 4;
+  if (cls == kClassSbh) scratch = sbh_warp_words<float>(sbh_r);
   return kTreeWords + kItemWords + (scratch + 3) / 4 * 4;
 }
 
+size_t class_smem(int cls, int bh_stack, int sbh_r) {
+  return (size_t)kEvalWarps * class_warp_words(cls, bh_stack, sbh_r) * sizeof(float);
+}
+
 template <int CLASS>
-void setup_class(size_t smem, int* per_sm) {
+void allow_smem(size_t smem) {
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(batch_eval_kernel<CLASS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
+}
+
+template <int CLASS>
+int occupancy(size_t smem) {
   int n = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_eval_kernel<CLASS>, kEvalThreads, smem);
-  *per_sm = std::max(1, n);
+  return std::max(1, n);
+}
+
+int class_occupancy(int cls, size_t smem) {
+  return cls == kClassBh ? occupancy<kClassBh>(smem)
+         : cls == kClassSbh ? occupancy<kClassSbh>(smem)
+                            : occupancy<kClassBf>(smem);
+}
+
+// Launch shapes are rounded so that few graphs serve every batch: the stack
+// to a multiple of 32 entries, the root width to a power of two from 64.
+// Shared memory sized to the batch (not to the engine's limits) leaves the
+// rest of each SM's 228 KB to the L1 cache the traversals depend on.
+int round_stack(int need, const BatchEngine::Limits& lim) {
+  return std::min((need + 31) / 32 * 32, lim.max_tree_depth + 2);
+}
+int round_root(int need, const BatchEngine::Limits& lim) {
+  int r = 64;
+  while (r < need) r *= 2;
+  return std::min(r, lim.max_root_children);
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -299,7 +401,8 @@ BatchEngine::BatchEngine(const Limits& lim, int sm_count) : lim_(lim), sm_count_
   const size_t o_keys = o_items + align256(sizeof(BatchItem) * lim_.max_items);
   const size_t o_hist = o_keys + align256(sizeof(unsigned) * lim_.max_queries);
   const size_t o_order = o_hist + align256(sizeof(unsigned) * nb);
-  dev_bytes_ = o_order + align256(sizeof(int) * lim_.max_queries);
+  const size_t o_qbox = o_order + align256(sizeof(int) * lim_.max_queries);
+  dev_bytes_ = o_qbox + align256(sizeof(unsigned) * 6 * lim_.max_items);
   if (cudaMalloc(&dev_, dev_bytes_) != cudaSuccess) {
     dev_ = nullptr;
     return;
@@ -310,13 +413,17 @@ BatchEngine::BatchEngine(const Limits& lim, int sm_count) : lim_(lim), sm_count_
   d_keys_ = reinterpret_cast<unsigned*>(b + o_keys);
   d_hist_ = reinterpret_cast<unsigned*>(b + o_hist);
   d_order_ = reinterpret_cast<int*>(b + o_order);
+  d_qbox_ = reinterpret_cast<unsigned*>(b + o_qbox);
   if (cudaMallocHost(&h_stage_, o_keys) != cudaSuccess) h_stage_ = nullptr;
-  // Per-warp shared memory of each class's kernel.
+  // Allow each class's kernel the shared memory of the engine's largest
+  // shape; report occupancy at the smallest (the register bound).
+  const int big_stack = lim_.max_tree_depth + 2, big_root = lim_.max_root_children;
+  allow_smem<kClassBh>(class_smem(kClassBh, big_stack, big_root));
+  allow_smem<kClassSbh>(class_smem(kClassSbh, big_stack, big_root));
+  allow_smem<kClassBf>(class_smem(kClassBf, big_stack, big_root));
+  const int small_stack = round_stack(0, lim_), small_root = round_root(0, lim_);
   for (int c = 0; c < kClasses; c++)
-    eval_smem_[c] = (size_t)kEvalWarps * class_warp_words(c, lim_) * sizeof(float);
-  setup_class<kClassBh>(eval_smem_[kClassBh], &per_sm_[kClassBh]);
-  setup_class<kClassSbh>(eval_smem_[kClassSbh], &per_sm_[kClassSbh]);
-  setup_class<kClassBf>(eval_smem_[kClassBf], &per_sm_[kClassBf]);
+    per_sm_[c] = class_occupancy(c, class_smem(c, small_stack, small_root));
 }
 
 BatchEngine::~BatchEngine() {
@@ -348,6 +455,8 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
     it.sort_bits =
         (sorted && it.sort_bits >= 0) ? sort_bits_for(it.nq, t.dim, tuning.bucket_queries) : 0;
     it.dim = t.dim;
+    it.depth = t.depth;
+    it.root_children = t.root_children;
     it.sort_base = sort_base;
     it.bucket_base = bucket_base;
     it.buckets = it.sort_bits > 0 ? (1LL << (t.dim * it.sort_bits)) : 1;
@@ -368,7 +477,7 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
   return "";
 }
 
-cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status, int per_sm_cap,
+cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status, const Shape& shape,
                                  cudaGraphExec_t* out) {
   *out = nullptr;
   // Captured on private streams (the caller's may be the legacy default
@@ -386,10 +495,12 @@ cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status, int per_
   if (e == cudaSuccess) e = cudaStreamBeginCapture(st[0], cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     const int aux_blocks = sm_count_ * 4;
-    const int stack_cap = lim_.max_tree_depth + 2;
+    const int stack_cap = shape.bh_stack;
     cudaMemsetAsync(d_hist_, 0, sizeof(unsigned) * max_buckets(lim_), st[0]);
-    batch_keys_kernel<<<aux_blocks, kAuxThreads, 0, st[0]>>>(d_header_, d_items_, d_keys_,
-                                                             d_hist_);
+    cudaMemsetAsync(d_qbox_, 0, sizeof(unsigned) * 6 * lim_.max_items, st[0]);
+    batch_bbox_kernel<<<aux_blocks, kAuxThreads, 0, st[0]>>>(d_header_, d_items_, d_qbox_);
+    batch_keys_kernel<<<aux_blocks, kAuxThreads, 0, st[0]>>>(d_header_, d_items_, d_qbox_,
+                                                             d_keys_, d_hist_);
     batch_scan_kernel<<<1, kScanThreads, 0, st[0]>>>(d_header_, d_hist_);
     batch_scatter_kernel<<<aux_blocks, kAuxThreads, 0, st[0]>>>(d_header_, d_items_, d_keys_,
                                                                 d_hist_, d_order_);
@@ -397,17 +508,19 @@ cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status, int per_
     for (int c = 0; c < kClasses; c++) {
       cudaStream_t s = c == 0 ? st[0] : st[c];
       if (c > 0) cudaStreamWaitEvent(s, ev[0], 0);
-      const int per_sm = per_sm_cap > 0 ? std::min(per_sm_cap, per_sm_[c]) : per_sm_[c];
+      const size_t smem = class_smem(c, shape.bh_stack, shape.sbh_root);
+      const int fit = class_occupancy(c, smem);
+      const int per_sm = shape.per_sm_cap > 0 ? std::min(shape.per_sm_cap, fit) : fit;
       const int blocks = per_sm * sm_count_;
-      const int words = class_warp_words(c, lim_);
+      const int words = class_warp_words(c, shape.bh_stack, shape.sbh_root);
       if (c == kClassBh)
-        batch_eval_kernel<kClassBh><<<blocks, kEvalThreads, eval_smem_[c], s>>>(
+        batch_eval_kernel<kClassBh><<<blocks, kEvalThreads, smem, s>>>(
             d_header_, d_items_, d_trees, d_order_, d_status, words, stack_cap);
       else if (c == kClassSbh)
-        batch_eval_kernel<kClassSbh><<<blocks, kEvalThreads, eval_smem_[c], s>>>(
+        batch_eval_kernel<kClassSbh><<<blocks, kEvalThreads, smem, s>>>(
             d_header_, d_items_, d_trees, d_order_, d_status, words, stack_cap);
       else
-        batch_eval_kernel<kClassBf><<<blocks, kEvalThreads, eval_smem_[c], s>>>(
+        batch_eval_kernel<kClassBf><<<blocks, kEvalThreads, smem, s>>>(
             d_header_, d_items_, d_trees, d_order_, d_status, words, stack_cap);
       if (c > 0) {
         cudaEventRecord(ev[c], s);
@@ -440,14 +553,23 @@ cudaError_t BatchEngine::launch(const std::vector<BatchItem>& items, const DevTr
     captured_trees_ = d_trees;
     captured_status_ = d_status;
   }
-  const int cap = std::max(0, tuning.blocks_per_sm);
+  int need_depth = 0, need_root = 0;
+  for (const BatchItem& it : items) {
+    const int c = batch_class(it.method);
+    if (c == kClassBh) need_depth = std::max(need_depth, it.depth);
+    if (c == kClassSbh) need_root = std::max(need_root, it.root_children);
+  }
+  Shape shape;
+  shape.per_sm_cap = std::max(0, tuning.blocks_per_sm);
+  shape.bh_stack = round_stack(need_depth + 2, lim_);
+  shape.sbh_root = round_root(need_root, lim_);
   cudaGraphExec_t exec = nullptr;
   for (const Graph& g : graphs_)
-    if (g.blocks == cap) exec = g.exec;
+    if (g.shape == shape) exec = g.exec;
   if (!exec) {
-    cudaError_t e = capture(d_trees, d_status, cap, &exec);
+    cudaError_t e = capture(d_trees, d_status, shape, &exec);
     if (e != cudaSuccess) return e;
-    graphs_.push_back(Graph{cap, exec});
+    graphs_.push_back(Graph{shape, exec});
   }
   BatchHeader h = {};
   h.n_items = (int)items.size();

@@ -23,6 +23,8 @@ struct BatchItem {
   float beta;                // Barnes-Hut
   int sort_bits;             // Morton bits per axis of the query bucketing (0: keep order)
   int unit_queries;          // queries per work unit
+  int depth;                 // the tree's depth and root width (size the launch's
+  int root_children;         // shared memory; the kernels read the tree record's)
   KParams kp;
   unsigned long long seed;   // stochastic method
   const float* q;            // device SoA [dim][nq]
@@ -37,7 +39,6 @@ struct BatchItem {
   long long buckets;         // buckets of this request
   long long unit_base;       // first work unit of this request within its class
   long long units;           // work units of this request
-  float box_lo[3], box_hi[3];  // Morton box (the tree's root AABB)
 };
 
 // Requests are evaluated by one persistent kernel per method class (each
@@ -100,23 +101,32 @@ class BatchEngine {
 
   const Limits& limits() const { return lim_; }
   size_t device_bytes() const { return dev_bytes_; }
-  // CTAs per SM of the evaluation kernels at full occupancy (the largest).
+  // CTAs per SM of the evaluation kernels at full occupancy (the largest, at
+  // the smallest launch shape).
   int max_blocks_per_sm() const {
     return std::max(per_sm_[0], std::max(per_sm_[1], per_sm_[2]));
   }
 
  private:
+  // What a captured pipeline is specialised for.
+  struct Shape {
+    int per_sm_cap = 0;  // the tuning's CTAs-per-SM cap (0: none)
+    int bh_stack = 0;    // Barnes-Hut stack entries per warp
+    int sbh_root = 0;    // widest sampler root the scratch holds
+    bool operator==(const Shape& o) const {
+      return per_sm_cap == o.per_sm_cap && bh_stack == o.bh_stack && sbh_root == o.sbh_root;
+    }
+  };
   struct Graph {
-    int blocks = 0;  // the tuning's CTAs-per-SM cap (0: none)
+    Shape shape;
     cudaGraphExec_t exec = nullptr;
   };
-  cudaError_t capture(const DevTree* d_trees, int* d_status, int per_sm_cap,
+  cudaError_t capture(const DevTree* d_trees, int* d_status, const Shape& shape,
                       cudaGraphExec_t* out);
 
   Limits lim_;
   int sm_count_;
-  int per_sm_[kClasses] = {1, 1, 1};
-  size_t eval_smem_[kClasses] = {0, 0, 0};
+  int per_sm_[kClasses] = {1, 1, 1};  // at the smallest launch shape
   // device buffers
   void* dev_ = nullptr;
   size_t dev_bytes_ = 0;
@@ -125,9 +135,10 @@ class BatchEngine {
   unsigned* d_keys_ = nullptr;
   unsigned* d_hist_ = nullptr;
   int* d_order_ = nullptr;
+  unsigned* d_qbox_ = nullptr;  // per request: its queries' bounding box
   // pinned staging of header + items
   void* h_stage_ = nullptr;
-  // captured pipelines, one per CTAs-per-SM cap
+  // captured pipelines, one per launch shape
   std::vector<Graph> graphs_;
   const DevTree* captured_trees_ = nullptr;
   int* captured_status_ = nullptr;

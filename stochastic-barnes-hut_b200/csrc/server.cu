@@ -55,10 +55,6 @@ BatchItem make_item(int tree_index, const sbh_gpu_tree* t, const sbh_params& p) 
   it.kp.alpha = std::isnan(p.alpha) ? t->dev.alpha : p.alpha;
   it.kp.eps2 = p.eps * p.eps;
   it.seed = p.seed;
-  for (int k = 0; k < 3; k++) {
-    it.box_lo[k] = t->box_lo[k];
-    it.box_hi[k] = t->box_hi[k];
-  }
   return it;
 }
 
