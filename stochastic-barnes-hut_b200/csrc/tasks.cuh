@@ -132,28 +132,30 @@ __device__ __forceinline__ typename A::V add_leaf_points(const DevTree& t, int4 
   return acc;
 }
 
-// Expansion of up to 32 internal nodes at once.  Lane l owns node `v` (topo tv)
-// when `own`.  The warp lays every owner's node and its children out as one
-// flat list of entries (owner by owner, each node followed by its children in
-// cell order) and walks it 32 entries at a time: lane r finds the owner of
-// entry r by a binary search over the owners' prefix counts (shuffles), loads
-// that node record (consecutive children: coalesced) and evaluates it -- a leaf
-// child with several points as the sum of its points
-// (include/tree_sampler.h:264-280).  A segmented inclusive scan across the
-// lanes (one segment per owner) adds each owner's children; the owner takes its
-// segment's total from the segment's last lane, and k(v) from its first.  So
-// the owner gets kv = k(v), the children sum, and `contribs`, the number of
-// kernel evaluations that sum stands for.  The children are added as a
-// balanced tree, not left to right: the result is the same sum to within FP32
-// rounding, and deterministic (it depends only on the query, the tree and the
-// random streams).  All lanes must call.
+// Expansion of up to 32 internal nodes at once: lane l owns node `v` (topo
+// tv) when `own` and receives the sum of k over v's children, and `contribs`,
+// the number of kernel evaluations that sum stands for.  The warp lays every
+// owner's children out as one flat list of entries (owner by owner, in cell
+// order) and walks it 32 entries at a time: lane r finds the owner of entry r
+// from the segment starts of the chunk (a bit mask) and the owners' order in
+// shared memory, loads that child's record (consecutive children: coalesced)
+// and evaluates it -- a leaf child with several points as the sum of its
+// points (include/tree_sampler.h:264-280).  A segmented inclusive scan across
+// the lanes (one segment per owner) adds each owner's children; the owner
+// takes its segment's total from the segment's last lane.  Children that stand
+// for one evaluation each (internal nodes, one-point leaves) need no count
+// scan: the owner counts its entries in the chunk, and the scan of counts runs
+// only for chunks holding a multi-point or empty leaf.  The children are added
+// as a balanced tree, not left to right: the result is the same sum to within
+// FP32 rounding, and deterministic (it depends only on the query, the tree and
+// the random streams).  Owners evaluate k(v) themselves.  All lanes must call.
 template <class A>
 __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int v, int4 tv,
                                                 float3 q, const KParams& kp, int lane,
-                                                int* ownlane, typename A::V& kv, int& contribs) {
+                                                int* ownlane, int& contribs) {
   using V = typename A::V;
   const unsigned full = 0xffffffffu;
-  const int nent = own ? tv.y + 1 : 0;
+  const int nent = own ? tv.y : 0;
   int incl = nent;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -166,61 +168,63 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
   const unsigned owners = __ballot_sync(full, own);
   if (own) ownlane[__popc(owners & ((1u << lane) - 1u))] = lane;
   __syncwarp();
+  // Entry e of owner o is child (tv.x + e - excl) of o.
+  const int node_off = tv.x - excl;
+  const unsigned upto = lane == 31 ? full : (2u << lane) - 1u;  // chunk positions 0..lane
   V acc = A::zero();
-  kv = A::zero();
   contribs = 0;
   for (int base = 0; base < total; base += 32) {
     const int e = base + lane;
     // Owner of entry e: the owner whose segment covers the chunk's first entry,
-    // advanced by the segments that start between there and e.
+    // advanced by the segments that start between there and e.  Every owner
+    // has at least one child, so segments are never empty.
     const unsigned starts =
         __reduce_or_sync(full, (own && excl >= base && excl < base + 32) ? 1u << (excl - base) : 0u);
     const int first = __popc(__ballot_sync(full, own && excl <= base)) - 1;
-    const int o = ownlane[min(first + __popc(starts & (((2u << lane) - 1u) & ~1u)), 31)];
-    const int o_excl = __shfl_sync(full, excl, o);
-    const int o_v = __shfl_sync(full, v, o);
-    const int o_first = __shfl_sync(full, tv.x, o);
-    const int k = e - o_excl;  // 0: the owner's node; 1..: its children
+    const int o = ownlane[min(first + __popc(starts & upto & ~1u), 31)];
+    const int o_off = __shfl_sync(full, node_off, o);
+    // Segment head: the last segment start at or before this lane (0: the
+    // segment runs on from the previous chunk).
+    const int head = max(31 - __clz(starts & upto), 0);
     V val = A::zero();
     int cnt = 0;
     if (e < total) {
-      const int node = k == 0 ? o_v : o_first + k - 1;
+      const int node = o_off + e;
       // Node record: an aggregate, or for a one-point leaf the point itself; a
       // negative diameter marks a leaf whose points must be summed.
       const float4 cm = __ldg(t.nd_cm + node);
       const float4 ag = __ldg(t.nd_agg + node);
-      if (k > 0 && cm.w < 0.f) {
+      if (cm.w < 0.f) {
         const int4 tc = __ldg(t.nd_topo + node);
         val = add_leaf_points<A>(t, tc, q, kp, A::zero());
         cnt = tc.w - tc.z;
       } else {
         val = A::node(cm, ag, q, kp);
-        cnt = k > 0 ? 1 : 0;
+        cnt = 1;
       }
     }
-    // Segmented inclusive scan of the children's values (the node's own entry
-    // contributes zero); segment head: the owner's first entry in this chunk.
-    const int head = max(o_excl - base, 0);
-    V x = k > 0 ? val : A::zero();
+    const bool counted = __any_sync(full, e < total && cnt != 1);
+    V x = val;
     int cx = cnt;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
       const V y = A::shfl_up(x, d);
-      const int cy = __shfl_up_sync(full, cx, d);
-      if (lane - d >= head) {
-        x = A::add(y, x);
-        cx += cy;
+      if (lane - d >= head) x = A::add(y, x);
+    }
+    if (counted) {
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int cy = __shfl_up_sync(full, cx, d);
+        if (lane - d >= head) cx += cy;
       }
     }
     const bool mine = own && excl < base + 32 && incl > base;
-    const int tail = mine ? min(incl, base + 32) - 1 - base : lane;
-    const V part = A::shfl(x, tail);
-    const int pc = __shfl_sync(full, cx, tail);
-    const V node_val = A::shfl(val, mine ? max(excl - base, 0) : lane);
+    const int last = mine ? min(incl, base + 32) - 1 - base : lane;
+    const V part = A::shfl(x, last);
+    const int pc = counted ? __shfl_sync(full, cx, last) : last + 1 - max(excl - base, 0);
     if (mine) {
       acc = A::add(acc, part);
       contribs += pc;
-      if (excl >= base) kv = node_val;
     }
   }
   return acc;
@@ -340,9 +344,10 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       cnt += tS.y != 0 ? 1 : tS.w - tS.z;
     }
     const bool own = have && tS.y != 0;
+    V kS = A::zero();
+    if (own) kS = A::node(__ldg(t.nd_cm + c0 + j), __ldg(t.nd_agg + c0 + j), q, kp);
     int cc;
-    V kS;
-    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, lane, ws.ownlane, kS, cc);
+    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, lane, ws.ownlane, cc);
     if (have) {
       ws.bhS[j] = kS;
       ws.diffS[j] = own ? A::sub(sumc, kS) : A::zero();
@@ -418,9 +423,9 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
         }
       }
       int cc;
-      V kprev;
-      const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, ws.ownlane, kprev, cc);
+      const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, ws.ownlane, cc);
       if (own) {
+        const V kprev = A::node(__ldg(t.nd_cm + prev), __ldg(t.nd_agg + prev), q, kp);
         wd = A::add(wd, A::scale(w, A::sub(sumc, kprev)));
         cnt += cc;
       }
