@@ -7,7 +7,7 @@
 //                         its request's query box, with a per-request bucket
 //                         count sized to the request (about 8 queries per
 //                         bucket);
-//   batch_scan_kernel     one exclusive scan over all requests' buckets (each
+//   scan (scan.cuh)       one exclusive scan over all requests' buckets (each
 //                         request's buckets follow the previous request's, so
 //                         the scan also places every request at its offset);
 //   batch_scatter_kernel  the sorted position of every query;
@@ -29,6 +29,7 @@
 #include <cstring>
 
 #include "batch.h"
+#include "scan.cuh"
 #include "tasks.cuh"
 
 namespace sbh {
@@ -37,7 +38,6 @@ namespace {
 constexpr int kEvalThreads = 128;
 constexpr int kEvalWarps = kEvalThreads / 32;
 constexpr int kAuxThreads = 256;
-constexpr int kScanThreads = 1024;
 
 __device__ __forceinline__ int find_item_by(const BatchItem* items, int n, long long v,
                                             long long BatchItem::*field) {
@@ -151,31 +151,6 @@ __global__ void batch_keys_kernel(const BatchHeader* __restrict__ hdr,
     const unsigned bucket = (unsigned)(it.bucket_base + key);
     keys[g] = bucket;
     atomicAdd(hist + bucket, 1u);
-  }
-}
-
-// Exclusive scan of hist[0, total_buckets) by one block.
-__global__ void __launch_bounds__(kScanThreads)
-    batch_scan_kernel(const BatchHeader* __restrict__ hdr, unsigned* hist) {
-  __shared__ unsigned s[kScanThreads];
-  const long long total = hdr->total_buckets;
-  const long long per = (total + kScanThreads - 1) / kScanThreads;
-  const long long b = threadIdx.x * per, e = min(total, b + per);
-  unsigned sum = 0;
-  for (long long k = b; k < e; k++) sum += hist[k];
-  s[threadIdx.x] = sum;
-  __syncthreads();
-  for (int off = 1; off < kScanThreads; off <<= 1) {
-    const unsigned v = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
-    __syncthreads();
-    s[threadIdx.x] += v;
-    __syncthreads();
-  }
-  unsigned run = s[threadIdx.x] - sum;
-  for (long long k = b; k < e; k++) {
-    const unsigned c = hist[k];
-    hist[k] = run;
-    run += c;
   }
 }
 
@@ -402,7 +377,8 @@ BatchEngine::BatchEngine(const Limits& lim, int sm_count) : lim_(lim), sm_count_
   const size_t o_hist = o_keys + align256(sizeof(unsigned) * lim_.max_queries);
   const size_t o_order = o_hist + align256(sizeof(unsigned) * nb);
   const size_t o_qbox = o_order + align256(sizeof(int) * lim_.max_queries);
-  dev_bytes_ = o_qbox + align256(sizeof(unsigned) * 6 * lim_.max_items);
+  const size_t o_sums = o_qbox + align256(sizeof(unsigned) * 6 * lim_.max_items);
+  dev_bytes_ = o_sums + align256(sizeof(unsigned) * scan_tiles_for(nb));
   if (cudaMalloc(&dev_, dev_bytes_) != cudaSuccess) {
     dev_ = nullptr;
     return;
@@ -414,6 +390,7 @@ BatchEngine::BatchEngine(const Limits& lim, int sm_count) : lim_(lim), sm_count_
   d_hist_ = reinterpret_cast<unsigned*>(b + o_hist);
   d_order_ = reinterpret_cast<int*>(b + o_order);
   d_qbox_ = reinterpret_cast<unsigned*>(b + o_qbox);
+  d_sums_ = reinterpret_cast<unsigned*>(b + o_sums);
   if (cudaMallocHost(&h_stage_, o_keys) != cudaSuccess) h_stage_ = nullptr;
   // Allow each class's kernel the shared memory of the engine's largest
   // shape; report occupancy at the smallest (the register bound).
@@ -501,7 +478,7 @@ cudaError_t BatchEngine::capture(const DevTree* d_trees, int* d_status, const Sh
     batch_bbox_kernel<<<aux_blocks, kAuxThreads, 0, st[0]>>>(d_header_, d_items_, d_qbox_);
     batch_keys_kernel<<<aux_blocks, kAuxThreads, 0, st[0]>>>(d_header_, d_items_, d_qbox_,
                                                              d_keys_, d_hist_);
-    batch_scan_kernel<<<1, kScanThreads, 0, st[0]>>>(d_header_, d_hist_);
+    launch_scan(d_hist_, &d_header_->total_buckets, 0, max_buckets(lim_), d_sums_, st[0]);
     batch_scatter_kernel<<<aux_blocks, kAuxThreads, 0, st[0]>>>(d_header_, d_items_, d_keys_,
                                                                 d_hist_, d_order_);
     cudaEventRecord(ev[0], st[0]);

@@ -136,6 +136,7 @@ class BatchEngine {
   unsigned* d_hist_ = nullptr;
   int* d_order_ = nullptr;
   unsigned* d_qbox_ = nullptr;  // per request: its queries' bounding box
+  unsigned* d_sums_ = nullptr;  // tile sums of the bucket scan
   // pinned staging of header + items
   void* h_stage_ = nullptr;
   // captured pipelines, one per launch shape

@@ -429,7 +429,7 @@ SBH_API int sbh_gpu_tree_check(sbh_gpu_tree* tree, void* stream_ptr) {
 
 static __device__ __align__(256) unsigned char g_static_scratch[
     ((size_t)SBH_STATIC_SCRATCH_MAX_QUERIES * sizeof(int) + 255) / 256 * 256 +  // query order
-    256 + ((size_t)1 << 18) * 4 + (size_t)SBH_STATIC_SCRATCH_MAX_QUERIES * 4];  // sort workspace
+    sbh::query_sort_workspace_bytes(SBH_STATIC_SCRATCH_MAX_QUERIES)];        // sort workspace
 
 namespace {
 

@@ -30,8 +30,14 @@ cudaError_t launch_gradient(const DevTree& t, int method, int kernel, const floa
 size_t gradient_smem_bytes(const DevTree& t, int kernel);
 
 // Spatial ordering of queries: order[i] is the i-th query in Morton-bucket
-// order.  `ws` must hold query_sort_workspace_bytes(nq) bytes.
-size_t query_sort_workspace_bytes(long long nq);
+// order.  `ws` must hold query_sort_workspace_bytes(nq) bytes: the query box
+// and the bucket scan's tile sums (1,280 B), 2^18 bucket counters, a key per
+// query.
+constexpr int kQuerySortBuckets = 1 << 18;
+constexpr size_t kQuerySortHeadBytes = 256 + 1024;
+constexpr size_t query_sort_workspace_bytes(long long nq) {
+  return kQuerySortHeadBytes + (size_t)kQuerySortBuckets * 4 + (size_t)(nq > 0 ? nq : 1) * 4;
+}
 cudaError_t launch_query_sort(const float* q, long long nq, int dim, void* ws, int* order,
                               cudaStream_t stream);
 

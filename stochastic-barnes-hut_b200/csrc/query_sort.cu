@@ -8,13 +8,13 @@
 // is independent of which warp evaluates it.
 #include "device_common.cuh"
 #include "launch.h"
+#include "scan.cuh"
 
 namespace sbh {
 namespace {
 
-constexpr int kBucketBits = 18;
-constexpr int kBuckets = 1 << kBucketBits;
-constexpr int kScanThreads = 1024;
+constexpr int kBuckets = kQuerySortBuckets;
+static_assert(scan_tiles_for(kBuckets) * 4 <= 1024, "tile sums must fit the workspace head");
 
 // Order-preserving map of floats to unsigned ints for atomicMin/Max.
 __device__ __forceinline__ unsigned float_to_ordered(float f) {
@@ -27,17 +27,18 @@ __device__ __forceinline__ float ordered_to_float(unsigned u) {
 
 struct Workspace {
   unsigned* box;   // [6] ordered min x,y,z then max x,y,z
+  unsigned* sums;  // [kBuckets / kScanTile] tile sums of the bucket scan
   unsigned* hist;  // [kBuckets]
   unsigned* keys;  // [nq]
 };
 
-Workspace carve(void* ws, long long nq) {
+Workspace carve(void* ws) {
   char* p = static_cast<char*>(ws);
   Workspace w;
   w.box = reinterpret_cast<unsigned*>(p);
-  w.hist = reinterpret_cast<unsigned*>(p + 256);
-  w.keys = reinterpret_cast<unsigned*>(p + 256 + (size_t)kBuckets * 4);
-  (void)nq;
+  w.sums = reinterpret_cast<unsigned*>(p + 256);
+  w.hist = reinterpret_cast<unsigned*>(p + kQuerySortHeadBytes);
+  w.keys = reinterpret_cast<unsigned*>(p + kQuerySortHeadBytes + (size_t)kBuckets * 4);
   return w;
 }
 
@@ -114,29 +115,6 @@ __global__ void key_kernel(const float* __restrict__ q, long long nq, int dim,
   }
 }
 
-// Exclusive scan of kBuckets counters by one block.
-__global__ void __launch_bounds__(kScanThreads) scan_kernel(unsigned* hist) {
-  constexpr int per = kBuckets / kScanThreads;
-  __shared__ unsigned s[kScanThreads];
-  unsigned* h = hist + threadIdx.x * per;
-  unsigned sum = 0;
-  for (int k = 0; k < per; k++) sum += h[k];
-  s[threadIdx.x] = sum;
-  __syncthreads();
-  for (int off = 1; off < kScanThreads; off <<= 1) {
-    const unsigned v = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
-    __syncthreads();
-    s[threadIdx.x] += v;
-    __syncthreads();
-  }
-  unsigned run = s[threadIdx.x] - sum;
-  for (int k = 0; k < per; k++) {
-    const unsigned c = h[k];
-    h[k] = run;
-    run += c;
-  }
-}
-
 __global__ void scatter_kernel(const unsigned* __restrict__ keys, long long nq, unsigned* hist,
                                int* order) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nq;
@@ -154,20 +132,16 @@ __global__ void fill_kernel(int* p, long long n, int v) {
 
 }  // namespace
 
-size_t query_sort_workspace_bytes(long long nq) {
-  return 256 + (size_t)kBuckets * 4 + (size_t)(nq > 0 ? nq : 1) * 4;
-}
-
 cudaError_t launch_query_sort(const float* q, long long nq, int dim, void* ws, int* order,
                               cudaStream_t stream) {
   if (nq <= 0) return cudaSuccess;
-  Workspace w = carve(ws, nq);
+  Workspace w = carve(ws);
   const int threads = 256;
   const unsigned grid = (unsigned)min((nq + threads - 1) / threads, 4096LL);
   init_kernel<<<256, 256, 0, stream>>>(w.box, w.hist);
   bbox_kernel<<<grid, threads, 0, stream>>>(q, nq, dim, w.box);
   key_kernel<<<grid, threads, 0, stream>>>(q, nq, dim, w.box, w.keys, w.hist);
-  scan_kernel<<<1, kScanThreads, 0, stream>>>(w.hist);
+  launch_scan(w.hist, nullptr, kBuckets, kBuckets, w.sums, stream);
   scatter_kernel<<<grid, threads, 0, stream>>>(w.keys, nq, w.hist, order);
   return cudaGetLastError();
 }
