@@ -219,14 +219,19 @@ typedef struct sbh_batch_tuning {
   int32_t blocks_per_sm;        /* persistent CTAs per SM; 0 = as many as fit (default) */
   int32_t bh_unit_queries;      /* Barnes-Hut queries per warp walk, 1..32 (default 32; the
                                    warp-vote method always uses 32) */
+  int32_t direct_queries;       /* sbh_eval_batch: stochastic requests of at least this many
+                                   queries run as their own sampler launches, on side streams
+                                   beside the batch graph (same results); 0 = never (default
+                                   65536) */
 } sbh_batch_tuning;
 void sbh_batch_tuning_init(sbh_batch_tuning* tuning);
 /* The tuning sbh_eval_batch uses on `device` (initially the defaults). */
 int sbh_batch_set_tuning(int device, const sbh_batch_tuning* tuning);
 int sbh_batch_get_tuning(int device, sbh_batch_tuning* tuning);
 /* Autotuner: evaluates the batch under candidate tunings -- coordinate descent
- * over CTAs per SM, sampler unit size, bucket size and Barnes-Hut queries per
- * warp walk (the per-lane vs per-warp balance of the walk), each candidate timed
+ * over CTAs per SM, sampler unit size, bucket size, Barnes-Hut queries per
+ * warp walk (the per-lane vs per-warp balance of the walk) and the direct-launch
+ * threshold of large stochastic requests, each candidate timed
  * `repeats` times on `stream` after one untimed run -- installs the fastest as
  * the device's tuning and returns it with its time and the starting tuning's
  * time (ms, median of the repeats).  Blocks until done; the output buffers

@@ -72,6 +72,9 @@ class BatchEngine {
     int bucket_queries = 8;   // target queries per Morton bucket
     int blocks_per_sm = 0;    // persistent CTAs per SM (0: as many as fit)
     int bh_unit = 32;         // Barnes-Hut queries per warp walk (1..32)
+    // Stochastic requests of at least this many queries leave the batch and
+    // run as single-call launches (0: never); read by the batch's caller.
+    int direct_queries = 65536;
   };
 
   struct Limits {

@@ -73,6 +73,16 @@ inline void bind_tree(sbh_gpu_tree* g, const TreeLayout& L) {
 // A copy of a device tree (its own allocation and status word), on its device.
 int clone_gpu_tree(const sbh_gpu_tree* src, sbh_gpu_tree** out);
 
+// Enqueues one stochastic evaluation of a batched request as its own launch of
+// the single-call sampler (query sort with scratch from the library's pool,
+// then stochastic_kernel): device pointers, `self_mass` optional, device
+// bounds reported to `status`.  Results equal the batch kernel's for the same
+// request (the random streams are keyed by query index).  The caller has
+// checked the parameters and made the tree's device current.
+int enqueue_stochastic_direct(const sbh_gpu_tree* tree, const sbh_params& p, const float* d_q,
+                              long long nq, float* d_out, int* d_contribs,
+                              const float* d_self_mass, int* d_status, cudaStream_t stream);
+
 // Makes `dev` current for the scope and restores the previous device.
 struct DeviceGuard {
   int prev = -1;

@@ -329,6 +329,42 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
   return sbh::ok();
 }
 
+int sbh::enqueue_stochastic_direct(const sbh_gpu_tree* tree, const sbh_params& p,
+                                   const float* d_q, long long nq, float* d_out, int* d_contribs,
+                                   const float* d_self_mass, int* d_status,
+                                   cudaStream_t stream) {
+  if (nq <= 0) return SBH_OK;
+  const sbh::DevTree& t = tree->dev;
+  sbh::KParams kp;
+  kp.alpha = std::isnan(p.alpha) ? t.alpha : p.alpha;
+  kp.eps2 = p.eps * p.eps;
+  void* tmp = nullptr;
+  const int* order = nullptr;
+  if (wants_sort(&p)) {
+    const size_t b_ord = align256((size_t)nq * sizeof(int));
+    cudaMemPool_t pool = nullptr;
+    int st = scratch_pool(tree->device, &pool);
+    if (st != SBH_OK) return st;
+    SBH_CK(cudaMallocFromPoolAsync(&tmp, b_ord + sbh::query_sort_workspace_bytes(nq), pool,
+                                   stream),
+           "cudaMallocFromPoolAsync(workspace)");
+    int* d_ord = static_cast<int*>(tmp);
+    cudaError_t e = sbh::launch_query_sort(d_q, nq, t.dim, static_cast<char*>(tmp) + b_ord,
+                                           d_ord, stream);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(tmp, stream);
+      return cuda_fail(e, "query sort");
+    }
+    order = d_ord;
+  }
+  cudaError_t e = sbh::launch_stochastic(t, p.kernel, d_q, nq, order, p.samples_per_subdomain,
+                                         p.seed, kp, d_out, d_contribs, d_status, stream,
+                                         tree->sm_count, d_self_mass);
+  if (tmp) cudaFreeAsync(tmp, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  return SBH_OK;
+}
+
 int sbh::clone_gpu_tree(const sbh_gpu_tree* src, sbh_gpu_tree** out) {
   *out = nullptr;
   DeviceGuard guard(src->device);

@@ -15,10 +15,13 @@ cudaError_t launch_barnes_hut(const DevTree& t, int kernel, bool vote, const flo
                               float* out, int* contribs, int* status, cudaStream_t stream,
                               int sm_count);
 
+// self_mass (optional, indexed like the queries): subtract each query's own
+// source term, as batched requests may ask.
 cudaError_t launch_stochastic(const DevTree& t, int kernel, const float* q, long long nq,
                               const int* order, int samples, unsigned long long seed,
                               const KParams& kp, float* out, int* contribs, int* status,
-                              cudaStream_t stream, int sm_count);
+                              cudaStream_t stream, int sm_count,
+                              const float* self_mass = nullptr);
 
 // Values and query-position gradients (adjoint.cu): method is SBH_METHOD_*,
 // kernel gravity, Plummer or smooth distance; grads is SoA [dim][nq] or null.

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(SBH_THREADS, 8)
     stochastic_kernel(DevTree t, const float* __restrict__ qsoa, long long nq,
                       const int* __restrict__ order, int samples, unsigned long long seed,
                       KParams kp, float* __restrict__ out, int* __restrict__ contribs,
-                      int* status) {
+                      int* status, const float* __restrict__ self_mass) {
   extern __shared__ float s_mem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -63,8 +63,10 @@ __global__ void __launch_bounds__(SBH_THREADS, 8)
     const long long qi = order ? (long long)__ldg(order + slot) : slot;
     float r;
     int c;
-    sbh_query<DIM, K>(t, load_query<DIM>(qsoa, nq, qi), qi, samples, seed, kp, ws, status, r, c);
+    const float3 q = load_query<DIM>(qsoa, nq, qi);
+    sbh_query<DIM, K>(t, q, qi, samples, seed, kp, ws, status, r, c);
     if (lane == 0) {
+      if (self_mass) r = rsub(r, self_term<DIM, K>(q, __ldg(self_mass + qi), kp));
       out[qi] = r;
       if (contribs) contribs[qi] = c;
     }
@@ -74,7 +76,8 @@ __global__ void __launch_bounds__(SBH_THREADS, 8)
 template <int DIM, int K>
 cudaError_t launch_sbh(const DevTree& t, const float* q, long long nq, const int* order,
                        int samples, unsigned long long seed, const KParams& kp, float* out,
-                       int* contribs, int* status, cudaStream_t stream, int sm_count) {
+                       int* contribs, int* status, cudaStream_t stream, int sm_count,
+                       const float* self_mass) {
   const size_t smem = (size_t)SBH_WARPS * sbh_warp_words<float>(t.root_children) * sizeof(float);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(stochastic_kernel<DIM, K>,
@@ -85,7 +88,7 @@ cudaError_t launch_sbh(const DevTree& t, const float* q, long long nq, const int
   const long long cap = (long long)sm_count * 64;
   if (blocks > cap) blocks = cap;
   stochastic_kernel<DIM, K><<<(unsigned)blocks, SBH_THREADS, smem, stream>>>(
-      t, q, nq, order, samples, seed, kp, out, contribs, status);
+      t, q, nq, order, samples, seed, kp, out, contribs, status, self_mass);
   return cudaGetLastError();
 }
 
@@ -94,9 +97,9 @@ cudaError_t launch_sbh(const DevTree& t, const float* q, long long nq, const int
 cudaError_t launch_stochastic(const DevTree& t, int kernel, const float* q, long long nq,
                               const int* order, int samples, unsigned long long seed,
                               const KParams& kp, float* out, int* contribs, int* status,
-                              cudaStream_t stream, int sm_count) {
+                              cudaStream_t stream, int sm_count, const float* self_mass) {
   if (nq <= 0) return cudaSuccess;
-  if (t.root_children == 0) {
+  if (t.root_children == 0 && !self_mass) {
     // A single-leaf tree has no subdomains: every estimate is 0
     // (include/tree_sampler.h:214 iterates over no children).
     cudaError_t e = cudaMemsetAsync(out, 0, (size_t)nq * sizeof(float), stream);
@@ -105,7 +108,8 @@ cudaError_t launch_stochastic(const DevTree& t, int kernel, const float* q, long
   }
 #define SBH_SBH_CASE(D, K)      \
   if (t.dim == D && kernel == K) \
-    return launch_sbh<D, K>(t, q, nq, order, samples, seed, kp, out, contribs, status, stream, sm_count);
+    return launch_sbh<D, K>(t, q, nq, order, samples, seed, kp, out, contribs, status, stream, \
+                            sm_count, self_mass);
   SBH_SBH_CASE(3, kGravity)
   SBH_SBH_CASE(3, kWindingNumber)
   SBH_SBH_CASE(3, kSmoothDist)

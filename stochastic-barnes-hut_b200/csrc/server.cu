@@ -90,7 +90,36 @@ struct BatchContext {
   int* d_status = nullptr;
   cudaEvent_t done = nullptr;
   bool pending = false;
+  // Side streams of the direct launches (forked from and joined back into the
+  // caller's stream): two, so that one launch's last wave overlaps the next.
+  static constexpr int kSide = 2;
+  cudaStream_t side[kSide] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kSide] = {};
 };
+
+// Creates the context's side streams and events once.
+int ensure_side_streams(BatchContext& ctx) {
+  if (ctx.fork) return SBH_OK;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < BatchContext::kSide && e == cudaSuccess; i++) {
+    e = cudaStreamCreateWithFlags(&ctx.side[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx.join[i], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx.fork, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    for (int i = 0; i < BatchContext::kSide; i++) {
+      if (ctx.side[i]) cudaStreamDestroy(ctx.side[i]);
+      if (ctx.join[i]) cudaEventDestroy(ctx.join[i]);
+      ctx.side[i] = nullptr;
+      ctx.join[i] = nullptr;
+    }
+    if (ctx.fork) cudaEventDestroy(ctx.fork);
+    ctx.fork = nullptr;
+    return sbh::cuda_fail(e, "batch side streams");
+  }
+  return SBH_OK;
+}
 
 BatchContext& batch_context(int device) {
   static BatchContext ctx[64];
@@ -103,6 +132,7 @@ BatchEngine::Tuning to_engine(const sbh_batch_tuning& t) {
   e.bucket_queries = t.bucket_queries;
   e.blocks_per_sm = t.blocks_per_sm;
   e.bh_unit = t.bh_unit_queries;
+  e.direct_queries = t.direct_queries;
   return e;
 }
 
@@ -112,6 +142,7 @@ sbh_batch_tuning from_engine(const BatchEngine::Tuning& e) {
   t.bucket_queries = e.bucket_queries;
   t.blocks_per_sm = e.blocks_per_sm;
   t.bh_unit_queries = e.bh_unit;
+  t.direct_queries = e.direct_queries;
   return t;
 }
 
@@ -125,6 +156,8 @@ int check_tuning(const sbh_batch_tuning* t) {
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "blocks_per_sm must be in [0, 64]");
   if (t->bh_unit_queries < 1 || t->bh_unit_queries > 32)
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "bh_unit_queries must be in [1, 32]");
+  if (t->direct_queries < 0)
+    return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "direct_queries must be >= 0");
   return SBH_OK;
 }
 
@@ -172,8 +205,8 @@ int retire_previous(BatchContext& ctx) {
 
 // Enqueues a checked batch on `stream` with `tuning` (context lock held, device current).
 int enqueue_batch(BatchContext& ctx, const sbh_batch_item* items, int n_items,
-                  const std::vector<const sbh_gpu_tree*>& uniq, long long total,
-                  cudaStream_t stream, const BatchEngine::Tuning& tuning) {
+                  const std::vector<const sbh_gpu_tree*>& uniq, cudaStream_t stream,
+                  const BatchEngine::Tuning& tuning) {
   int st = retire_previous(ctx);
   if (st != SBH_OK) return st;
   // Tree table.
@@ -198,9 +231,33 @@ int enqueue_batch(BatchContext& ctx, const sbh_batch_item* items, int n_items,
   }
   if (!ctx.done && cudaEventCreateWithFlags(&ctx.done, cudaEventDisableTiming) != cudaSuccess)
     return sbh::fail(SBH_ERR_CUDA, "cudaEventCreate");
-  // Engine large enough for this batch (grown with headroom when it is not).
-  BatchEngine::Limits need = limits_for(table, n_items, total);
-  if (!ctx.engine || !covers(ctx.engine->limits(), need)) {
+  // Requests of the batch graph, and large stochastic requests run directly.
+  std::vector<BatchItem> plan;
+  std::vector<const sbh_batch_item*> direct;
+  plan.reserve(n_items);
+  long long batched = 0;
+  for (int i = 0; i < n_items; i++) {
+    const sbh_batch_item& b = items[i];
+    if (b.nq == 0) continue;
+    if (tuning.direct_queries > 0 && b.params.method == SBH_METHOD_STOCHASTIC &&
+        b.nq >= tuning.direct_queries) {
+      direct.push_back(&b);
+      continue;
+    }
+    const int ti = (int)(std::find(uniq.begin(), uniq.end(), b.tree) - uniq.begin());
+    BatchItem it = make_item(ti, b.tree, b.params);
+    it.q = b.d_queries;
+    it.out = b.d_results;
+    it.contribs = b.d_contribs;
+    it.self_mass = b.d_self_mass;
+    it.nq = b.nq;
+    plan.push_back(it);
+    batched += b.nq;
+  }
+  if (plan.empty() && direct.empty()) return SBH_OK;
+  // Engine large enough for the graph's requests (grown with headroom when it is not).
+  BatchEngine::Limits need = limits_for(table, (int)plan.size(), batched);
+  if (!plan.empty() && (!ctx.engine || !covers(ctx.engine->limits(), need))) {
     BatchEngine::Limits grow = need;
     if (ctx.engine) {
       const BatchEngine::Limits& o = ctx.engine->limits();
@@ -218,28 +275,50 @@ int enqueue_batch(BatchContext& ctx, const sbh_batch_item* items, int n_items,
       return sbh::fail(SBH_ERR_OUT_OF_MEMORY, "batch engine buffers");
     }
   }
-  std::vector<BatchItem> plan;
-  plan.reserve(n_items);
-  for (int i = 0; i < n_items; i++) {
-    const sbh_batch_item& b = items[i];
-    if (b.nq == 0) continue;
-    const int ti = (int)(std::find(uniq.begin(), uniq.end(), b.tree) - uniq.begin());
-    BatchItem it = make_item(ti, b.tree, b.params);
-    it.q = b.d_queries;
-    it.out = b.d_results;
-    it.contribs = b.d_contribs;
-    it.self_mass = b.d_self_mass;
-    it.nq = b.nq;
-    plan.push_back(it);
+  cudaError_t e = cudaSuccess;
+  // Large stochastic requests: their own launches of the single-call sampler,
+  // which keeps its tree record in kernel parameters (the batch kernel reads
+  // it from shared memory), on side streams forked here -- they read only the
+  // caller's inputs -- so that they overlap the batch graph and each other.
+  if (!direct.empty()) {
+    st = ensure_side_streams(ctx);
+    if (st != SBH_OK) return st;
+    e = cudaEventRecord(ctx.fork, stream);
+    for (int i = 0; i < BatchContext::kSide && e == cudaSuccess; i++)
+      e = cudaStreamWaitEvent(ctx.side[i], ctx.fork, 0);
+    if (e != cudaSuccess) return sbh::cuda_fail(e, "batch fork");  // nothing launched yet
+    for (size_t k = 0; k < direct.size(); k++) {
+      const sbh_batch_item* b = direct[k];
+      st = sbh::enqueue_stochastic_direct(b->tree, b->params, b->d_queries, b->nq, b->d_results,
+                                          b->d_contribs, b->d_self_mass, ctx.d_status,
+                                          ctx.side[k % BatchContext::kSide]);
+      if (st != SBH_OK) break;
+    }
   }
-  if (plan.empty()) return SBH_OK;
-  std::string err = ctx.engine->plan(plan, table, tuning);
-  if (!err.empty()) return sbh::fail(SBH_ERR_INVALID_ARGUMENT, err);
-  std::memcpy(ctx.h_trees, table.data(), sizeof(DevTree) * table.size());
-  cudaError_t e = cudaMemcpyAsync(ctx.d_trees, ctx.h_trees, sizeof(DevTree) * table.size(),
-                                  cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess) e = ctx.engine->launch(plan, ctx.d_trees, ctx.d_status, stream, tuning);
-  if (e == cudaSuccess) e = cudaEventRecord(ctx.done, stream);
+  if (st == SBH_OK && !plan.empty()) {
+    std::string err = ctx.engine->plan(plan, table, tuning);
+    if (!err.empty()) {
+      st = sbh::fail(SBH_ERR_INVALID_ARGUMENT, err);
+    } else {
+      std::memcpy(ctx.h_trees, table.data(), sizeof(DevTree) * table.size());
+      e = cudaMemcpyAsync(ctx.d_trees, ctx.h_trees, sizeof(DevTree) * table.size(),
+                          cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess)
+        e = ctx.engine->launch(plan, ctx.d_trees, ctx.d_status, stream, tuning);
+      if (e != cudaSuccess) st = sbh::cuda_fail(e, "batch launch");
+    }
+  }
+  // Join the side streams, also after a failure, so that the caller's stream
+  // never runs ahead of launches already made.
+  if (!direct.empty()) {
+    for (int i = 0; i < BatchContext::kSide; i++) {
+      e = cudaEventRecord(ctx.join[i], ctx.side[i]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, ctx.join[i], 0);
+      if (e != cudaSuccess && st == SBH_OK) st = sbh::cuda_fail(e, "batch join");
+    }
+  }
+  if (st != SBH_OK) return st;
+  e = cudaEventRecord(ctx.done, stream);
   if (e != cudaSuccess) return sbh::cuda_fail(e, "batch launch");
   ctx.pending = true;
   return SBH_OK;
@@ -257,7 +336,7 @@ SBH_API int sbh_eval_batch(const sbh_batch_item* items, int n_items, void* strea
   BatchContext& ctx = batch_context(device);
   std::lock_guard<std::mutex> lock(ctx.mu);
   sbh::DeviceGuard guard(device);
-  st = enqueue_batch(ctx, items, n_items, uniq, total, static_cast<cudaStream_t>(stream_ptr),
+  st = enqueue_batch(ctx, items, n_items, uniq, static_cast<cudaStream_t>(stream_ptr),
                      ctx.tuning);
   return st == SBH_OK ? sbh::ok() : st;
 }
@@ -307,14 +386,14 @@ SBH_API int sbh_batch_autotune(const sbh_batch_item* items, int n_items, void* s
   }
   // Median device time of `repeats` runs after one untimed run.
   auto time_of = [&](const BatchEngine::Tuning& t, float* ms) -> int {
-    int s = enqueue_batch(ctx, items, n_items, uniq, total, stream, t);
+    int s = enqueue_batch(ctx, items, n_items, uniq, stream, t);
     if (s != SBH_OK) return s;
     std::vector<float> v;
     for (int r = 0; r < repeats; r++) {
       s = retire_previous(ctx);
       if (s != SBH_OK) return s;
       cudaEventRecord(e0, stream);
-      s = enqueue_batch(ctx, items, n_items, uniq, total, stream, t);
+      s = enqueue_batch(ctx, items, n_items, uniq, stream, t);
       if (s != SBH_OK) return s;
       cudaEventRecord(e1, stream);
       cudaError_t e = cudaEventSynchronize(e1);
@@ -335,7 +414,7 @@ SBH_API int sbh_batch_autotune(const sbh_batch_item* items, int n_items, void* s
   const float first_ms = cur_ms;
   // Coordinate descent; a candidate must win by 2% to replace the incumbent.
   const int max_bps = ctx.engine ? ctx.engine->max_blocks_per_sm() : 1;
-  for (int coord = 0; coord < 4 && st == SBH_OK; coord++) {
+  for (int coord = 0; coord < 5 && st == SBH_OK; coord++) {
     std::vector<int> values;
     if (coord == 0) {
       for (int v : {0, max_bps * 3 / 4, max_bps / 2, max_bps / 4})
@@ -346,8 +425,10 @@ SBH_API int sbh_batch_autotune(const sbh_batch_item* items, int n_items, void* s
       values = {1, 2, 4, 8};
     } else if (coord == 2) {
       values = {4, 8, 16, 32};
-    } else {
+    } else if (coord == 3) {
       values = {32, 16, 8};
+    } else {
+      values = {0, 16384, 65536, 262144};
     }
     BatchEngine::Tuning best_t = cur;
     float best_t_ms = cur_ms;
@@ -356,7 +437,8 @@ SBH_API int sbh_batch_autotune(const sbh_batch_item* items, int n_items, void* s
       int& field = coord == 0   ? t.blocks_per_sm
                    : coord == 1 ? t.sampler_unit
                    : coord == 2 ? t.bucket_queries
-                                : t.bh_unit;
+                   : coord == 3 ? t.bh_unit
+                                : t.direct_queries;
       if (field == v) continue;
       field = v;
       float ms = 0.f;

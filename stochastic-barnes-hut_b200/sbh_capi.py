@@ -104,12 +104,13 @@ class BatchItem(ctypes.Structure):
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("sampler_unit_queries", ctypes.c_int32), ("bucket_queries", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("bh_unit_queries", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_int32), ("bh_unit_queries", ctypes.c_int32),
+                ("direct_queries", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {"sampler_unit_queries": self.sampler_unit_queries,
                 "bucket_queries": self.bucket_queries, "blocks_per_sm": self.blocks_per_sm,
-                "bh_unit_queries": self.bh_unit_queries}
+                "bh_unit_queries": self.bh_unit_queries, "direct_queries": self.direct_queries}
 
 
 class ServerConfig(ctypes.Structure):
@@ -394,7 +395,7 @@ def eval_batch(entries, stream: int = 0):
 
 
 def batch_tuning(sampler_unit_queries=None, bucket_queries=None, blocks_per_sm=None,
-                 bh_unit_queries=None) -> BatchTuning:
+                 bh_unit_queries=None, direct_queries=None) -> BatchTuning:
     """A tuning with the library defaults, overridden where given."""
     t = BatchTuning()
     lib().sbh_batch_tuning_init(ctypes.byref(t))
@@ -406,6 +407,8 @@ def batch_tuning(sampler_unit_queries=None, bucket_queries=None, blocks_per_sm=N
         t.blocks_per_sm = blocks_per_sm
     if bh_unit_queries is not None:
         t.bh_unit_queries = bh_unit_queries
+    if direct_queries is not None:
+        t.direct_queries = direct_queries
     return t
 
 

@@ -186,7 +186,8 @@ def test_batch_results_do_not_depend_on_tuning(env):
         for t in (C.batch_tuning(), C.batch_tuning(sampler_unit_queries=1, bucket_queries=32),
                   C.batch_tuning(sampler_unit_queries=8, bucket_queries=2, blocks_per_sm=1,
                                  bh_unit_queries=8),
-                  C.batch_tuning(bh_unit_queries=3)):
+                  C.batch_tuning(bh_unit_queries=3), C.batch_tuning(direct_queries=1),
+                  C.batch_tuning(direct_queries=0)):
             C.set_batch_tuning(t)
             for _, out, _ in keep:
                 out.zero_()
@@ -204,6 +205,54 @@ def test_batch_results_do_not_depend_on_tuning(env):
         C.set_batch_tuning(C.batch_tuning(bucket_queries=1))
     with pytest.raises(C.SbhError):
         C.set_batch_tuning(C.batch_tuning(bh_unit_queries=33))
+    with pytest.raises(C.SbhError):
+        C.set_batch_tuning(C.batch_tuning(direct_queries=-1))
+
+
+def test_direct_stochastic_requests_equal_batched(env):
+    """Stochastic requests at or above the tuning's direct_queries leave the
+    batch graph for their own sampler launches on side streams: values, counts
+    and the self-term subtraction must not change."""
+    torch, trees, gpus = env
+    pts, m = trees["gauss1_pts"]
+    stream = torch.cuda.current_stream().cuda_stream
+    reqs = []
+    for nq, self_mass in ((3000, True), (777, False), (40, True)):
+        dq = _dev(torch, pts[:nq])
+        dm = torch.from_numpy(np.ascontiguousarray(m[:nq])).cuda()
+        out = torch.empty(nq, dtype=torch.float32, device="cuda")
+        cnt = torch.empty(nq, dtype=torch.int32, device="cuda")
+        reqs.append((nq, dq, dm if self_mass else None, out, cnt))
+    p = C.params(method=C.STOCHASTIC, kernel=C.GRAVITY, samples_per_subdomain=3, seed=11)
+    bh = C.params(method=C.BARNES_HUT, kernel=C.GRAVITY, beta=2.0)
+    bh_out = torch.empty(500, dtype=torch.float32, device="cuda")
+    default = C.get_batch_tuning()
+    results = []
+    try:
+        for direct in (0, 1, 500):
+            C.set_batch_tuning(C.batch_tuning(direct_queries=direct))
+            entries = [(gpus["gauss1"], p, dq.data_ptr(), nq, out.data_ptr(), cnt.data_ptr(),
+                        dm.data_ptr() if dm is not None else 0)
+                       for nq, dq, dm, out, cnt in reqs]
+            entries.append((gpus["gauss1"], bh, reqs[0][1].data_ptr(), 500, bh_out.data_ptr(), 0,
+                            0))
+            for _, _, _, out, cnt in reqs:
+                out.fill_(float("nan"))
+                cnt.fill_(-1)
+            C.eval_batch(entries, stream=stream)
+            torch.cuda.synchronize()
+            results.append([(out.cpu().numpy().copy(), cnt.cpu().numpy().copy())
+                            for _, _, _, out, cnt in reqs])
+    finally:
+        C.set_batch_tuning(default)
+    for other in results[1:]:
+        for (a, ca), (b, cb) in zip(results[0], other):
+            assert bits_equal(a, b)
+            assert np.array_equal(ca, cb)
+    # the request without self terms equals a plain call
+    want, _, wcnt = gpus["gauss1"].eval(pts[:777], p, contribs=True)
+    assert bits_equal(results[1][1][0], want)
+    assert np.array_equal(results[1][1][1], wcnt)
 
 
 def test_autotune_installs_a_valid_tuning(env):
