@@ -76,12 +76,14 @@ int clone_gpu_tree(const sbh_gpu_tree* src, sbh_gpu_tree** out);
 // Enqueues one stochastic evaluation of a batched request as its own launch of
 // the single-call sampler (query sort with scratch from the library's pool,
 // then stochastic_kernel): device pointers, `self_mass` optional, device
-// bounds reported to `status`.  Results equal the batch kernel's for the same
-// request (the random streams are keyed by query index).  The caller has
-// checked the parameters and made the tree's device current.
+// bounds reported to `status`, `query_base` the index of d_q's first query in
+// its whole request.  Results equal the batch kernel's for the same request
+// (the random streams are keyed by query index).  The caller has checked the
+// parameters and made the tree's device current.
 int enqueue_stochastic_direct(const sbh_gpu_tree* tree, const sbh_params& p, const float* d_q,
                               long long nq, float* d_out, int* d_contribs,
-                              const float* d_self_mass, int* d_status, cudaStream_t stream);
+                              const float* d_self_mass, int* d_status, cudaStream_t stream,
+                              long long query_base = 0);
 
 // Makes `dev` current for the scope and restores the previous device.
 struct DeviceGuard {

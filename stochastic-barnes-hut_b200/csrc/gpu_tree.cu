@@ -332,7 +332,7 @@ SBH_API int sbh_gpu_tree_create(const sbh_host_tree* host, int device, sbh_gpu_t
 int sbh::enqueue_stochastic_direct(const sbh_gpu_tree* tree, const sbh_params& p,
                                    const float* d_q, long long nq, float* d_out, int* d_contribs,
                                    const float* d_self_mass, int* d_status,
-                                   cudaStream_t stream) {
+                                   cudaStream_t stream, long long query_base) {
   if (nq <= 0) return SBH_OK;
   const sbh::DevTree& t = tree->dev;
   sbh::KParams kp;
@@ -359,7 +359,7 @@ int sbh::enqueue_stochastic_direct(const sbh_gpu_tree* tree, const sbh_params& p
   }
   cudaError_t e = sbh::launch_stochastic(t, p.kernel, d_q, nq, order, p.samples_per_subdomain,
                                          p.seed, kp, d_out, d_contribs, d_status, stream,
-                                         tree->sm_count, d_self_mass);
+                                         tree->sm_count, d_self_mass, query_base);
   if (tmp) cudaFreeAsync(tmp, stream);
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   return SBH_OK;

@@ -16,12 +16,13 @@ cudaError_t launch_barnes_hut(const DevTree& t, int kernel, bool vote, const flo
                               int sm_count);
 
 // self_mass (optional, indexed like the queries): subtract each query's own
-// source term, as batched requests may ask.
+// source term, as batched requests may ask.  query_base: index of q[0] within
+// its whole request (keys the random streams of a request split into parts).
 cudaError_t launch_stochastic(const DevTree& t, int kernel, const float* q, long long nq,
                               const int* order, int samples, unsigned long long seed,
                               const KParams& kp, float* out, int* contribs, int* status,
                               cudaStream_t stream, int sm_count,
-                              const float* self_mass = nullptr);
+                              const float* self_mass = nullptr, long long query_base = 0);
 
 // Values and query-position gradients (adjoint.cu): method is SBH_METHOD_*,
 // kernel gravity, Plummer or smooth distance; grads is SoA [dim][nq] or null.

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(SBH_THREADS, 8)
     stochastic_kernel(DevTree t, const float* __restrict__ qsoa, long long nq,
                       const int* __restrict__ order, int samples, unsigned long long seed,
                       KParams kp, float* __restrict__ out, int* __restrict__ contribs,
-                      int* status, const float* __restrict__ self_mass) {
+                      int* status, const float* __restrict__ self_mass, long long query_base) {
   extern __shared__ float s_mem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(SBH_THREADS, 8)
     float r;
     int c;
     const float3 q = load_query<DIM>(qsoa, nq, qi);
-    sbh_query<DIM, K>(t, q, qi, samples, seed, kp, ws, status, r, c);
+    sbh_query<DIM, K>(t, q, query_base + qi, samples, seed, kp, ws, status, r, c);
     if (lane == 0) {
       if (self_mass) r = rsub(r, self_term<DIM, K>(q, __ldg(self_mass + qi), kp));
       out[qi] = r;
@@ -77,7 +77,7 @@ template <int DIM, int K>
 cudaError_t launch_sbh(const DevTree& t, const float* q, long long nq, const int* order,
                        int samples, unsigned long long seed, const KParams& kp, float* out,
                        int* contribs, int* status, cudaStream_t stream, int sm_count,
-                       const float* self_mass) {
+                       const float* self_mass, long long query_base) {
   const size_t smem = (size_t)SBH_WARPS * sbh_warp_words<float>(t.root_children) * sizeof(float);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(stochastic_kernel<DIM, K>,
@@ -88,7 +88,7 @@ cudaError_t launch_sbh(const DevTree& t, const float* q, long long nq, const int
   const long long cap = (long long)sm_count * 64;
   if (blocks > cap) blocks = cap;
   stochastic_kernel<DIM, K><<<(unsigned)blocks, SBH_THREADS, smem, stream>>>(
-      t, q, nq, order, samples, seed, kp, out, contribs, status, self_mass);
+      t, q, nq, order, samples, seed, kp, out, contribs, status, self_mass, query_base);
   return cudaGetLastError();
 }
 
@@ -97,7 +97,8 @@ cudaError_t launch_sbh(const DevTree& t, const float* q, long long nq, const int
 cudaError_t launch_stochastic(const DevTree& t, int kernel, const float* q, long long nq,
                               const int* order, int samples, unsigned long long seed,
                               const KParams& kp, float* out, int* contribs, int* status,
-                              cudaStream_t stream, int sm_count, const float* self_mass) {
+                              cudaStream_t stream, int sm_count, const float* self_mass,
+                              long long query_base) {
   if (nq <= 0) return cudaSuccess;
   if (t.root_children == 0 && !self_mass) {
     // A single-leaf tree has no subdomains: every estimate is 0
@@ -109,7 +110,7 @@ cudaError_t launch_stochastic(const DevTree& t, int kernel, const float* q, long
 #define SBH_SBH_CASE(D, K)      \
   if (t.dim == D && kernel == K) \
     return launch_sbh<D, K>(t, q, nq, order, samples, seed, kp, out, contribs, status, stream, \
-                            sm_count, self_mass);
+                            sm_count, self_mass, query_base);
   SBH_SBH_CASE(3, kGravity)
   SBH_SBH_CASE(3, kWindingNumber)
   SBH_SBH_CASE(3, kSmoothDist)

@@ -548,7 +548,19 @@ int sbh_server::launch(int si) {
     s.engine.reset(new BatchEngine(need, sm_count));
     if (s.engine->device_bytes() == 0) return SBH_ERR_OUT_OF_MEMORY;
   }
+  // Large stochastic parts run as their own sampler launches on the slot's
+  // stream (as in sbh_eval_batch), the rest in the slot's batch graph.
+  struct Direct {
+    const sbh_gpu_tree* tree;
+    const sbh_params* p;
+    const float* q;
+    int64_t nq;
+    float* out;
+    int* cnt;
+    int64_t base;
+  };
   std::vector<BatchItem> items;
+  std::vector<Direct> direct;
   items.reserve(s.work.size());
   int64_t total = 0;
   s.want_counts = false;
@@ -566,15 +578,28 @@ int sbh_server::launch(int si) {
     it.nq = a.count;
     it.query_base = a.offset;
     s.want_counts = s.want_counts || r.contribs;
-    items.push_back(it);
+    if (cfg.tuning.direct_queries > 0 && r.p.method == SBH_METHOD_STOCHASTIC &&
+        a.count >= cfg.tuning.direct_queries)
+      direct.push_back(Direct{t, &r.p, it.q, a.count, it.out, it.contribs, a.offset});
+    else
+      items.push_back(it);
     total = a.slot_offset + a.count;
   }
   const BatchEngine::Tuning tuning = to_engine(cfg.tuning);
-  std::string err = s.engine->plan(items, h_trees, tuning);
-  if (!err.empty()) return SBH_ERR_INVALID_ARGUMENT;
+  if (!items.empty()) {
+    std::string err = s.engine->plan(items, h_trees, tuning);
+    if (!err.empty()) return SBH_ERR_INVALID_ARGUMENT;
+  }
   cudaError_t e = cudaMemcpyAsync(s.d_q, s.h_q, sizeof(float) * 3 * total, cudaMemcpyHostToDevice,
                                   s.stream);
-  if (e == cudaSuccess) e = s.engine->launch(items, d_trees, s.d_status, s.stream, tuning);
+  if (e == cudaSuccess && !items.empty())
+    e = s.engine->launch(items, d_trees, s.d_status, s.stream, tuning);
+  for (const Direct& d : direct) {
+    if (e != cudaSuccess) break;
+    if (sbh::enqueue_stochastic_direct(d.tree, *d.p, d.q, d.nq, d.out, d.cnt, nullptr, s.d_status,
+                                       s.stream, d.base) != SBH_OK)
+      e = cudaErrorLaunchFailure;
+  }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s.h_out, s.d_out, sizeof(float) * total, cudaMemcpyDeviceToHost, s.stream);
   if (e == cudaSuccess && s.want_counts)

@@ -291,3 +291,29 @@ def test_server_with_a_tuning(env):
     server.close()
     with pytest.raises(C.SbhError):
         C.Server(slots=1, slot_queries=1024, tuning=C.batch_tuning(bucket_queries=0))
+
+
+def test_server_direct_stochastic_parts(env):
+    """A stochastic request split across slots, every part at or above
+    direct_queries (own sampler launches keyed by the part's offset in the
+    request), next to a Barnes-Hut request in the slot graphs: both equal
+    single calls, values and counts."""
+    torch, trees, gpus = env
+    t = C.batch_tuning(direct_queries=1024)
+    server = C.Server(slots=2, slot_queries=4096, tuning=t)
+    tid = server.add_tree(trees["torus2"])
+    rng = np.random.default_rng(99)
+    q = rng.uniform(-1.2, 1.2, (10000, 3)).astype(np.float32)
+    qb = rng.uniform(-1.2, 1.2, (700, 3)).astype(np.float32)
+    p = C.params(method=C.STOCHASTIC, kernel=C.WINDING_NUMBER, samples_per_subdomain=2, seed=8)
+    pb = C.params(method=C.BARNES_HUT, kernel=C.WINDING_NUMBER, beta=2.0)
+    r = server.submit(tid, q, p, contribs=True)
+    rb = server.submit(tid, qb, pb)
+    got = r.wait()
+    cnt = r.contribs
+    want, _, wcnt = gpus["torus2"].eval(q, p, contribs=True)
+    assert bits_equal(got, want)
+    assert np.array_equal(cnt, wcnt)
+    wantb, _ = gpus["torus2"].eval(qb, pb)
+    assert bits_equal(rb.wait(), wantb)
+    server.close()
