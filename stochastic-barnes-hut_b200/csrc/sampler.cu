@@ -47,7 +47,11 @@ namespace {
 constexpr int SBH_THREADS = 128;
 constexpr int SBH_WARPS = SBH_THREADS / 32;
 
-template <int DIM, int K>
+// PART: the launch evaluates part of a batched request -- its random streams
+// are keyed by query_base + the query's index, and self_mass (when non-null)
+// subtracts each query's own source term.  Compiled apart so that plain calls
+// carry nothing of it.
+template <int DIM, int K, bool PART>
 __global__ void __launch_bounds__(SBH_THREADS, 8)
     stochastic_kernel(DevTree t, const float* __restrict__ qsoa, long long nq,
                       const int* __restrict__ order, int samples, unsigned long long seed,
@@ -64,13 +68,32 @@ __global__ void __launch_bounds__(SBH_THREADS, 8)
     float r;
     int c;
     const float3 q = load_query<DIM>(qsoa, nq, qi);
-    sbh_query<DIM, K>(t, q, query_base + qi, samples, seed, kp, ws, status, r, c);
+    sbh_query<DIM, K>(t, q, PART ? query_base + qi : qi, samples, seed, kp, ws, status, r, c);
     if (lane == 0) {
-      if (self_mass) r = rsub(r, self_term<DIM, K>(q, __ldg(self_mass + qi), kp));
+      if (PART && self_mass) r = rsub(r, self_term<DIM, K>(q, __ldg(self_mass + qi), kp));
       out[qi] = r;
       if (contribs) contribs[qi] = c;
     }
   }
+}
+
+template <int DIM, int K, bool PART>
+cudaError_t launch_sbh_variant(const DevTree& t, const float* q, long long nq, const int* order,
+                       int samples, unsigned long long seed, const KParams& kp, float* out,
+                       int* contribs, int* status, cudaStream_t stream, int sm_count,
+                       const float* self_mass, long long query_base) {
+  const size_t smem = (size_t)SBH_WARPS * sbh_warp_words<float>(t.root_children) * sizeof(float);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(stochastic_kernel<DIM, K, PART>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  long long blocks = (nq + SBH_WARPS - 1) / SBH_WARPS;
+  const long long cap = (long long)sm_count * 64;
+  if (blocks > cap) blocks = cap;
+  stochastic_kernel<DIM, K, PART><<<(unsigned)blocks, SBH_THREADS, smem, stream>>>(
+      t, q, nq, order, samples, seed, kp, out, contribs, status, self_mass, query_base);
+  return cudaGetLastError();
 }
 
 template <int DIM, int K>
@@ -78,18 +101,11 @@ cudaError_t launch_sbh(const DevTree& t, const float* q, long long nq, const int
                        int samples, unsigned long long seed, const KParams& kp, float* out,
                        int* contribs, int* status, cudaStream_t stream, int sm_count,
                        const float* self_mass, long long query_base) {
-  const size_t smem = (size_t)SBH_WARPS * sbh_warp_words<float>(t.root_children) * sizeof(float);
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(stochastic_kernel<DIM, K>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  long long blocks = (nq + SBH_WARPS - 1) / SBH_WARPS;
-  const long long cap = (long long)sm_count * 64;
-  if (blocks > cap) blocks = cap;
-  stochastic_kernel<DIM, K><<<(unsigned)blocks, SBH_THREADS, smem, stream>>>(
-      t, q, nq, order, samples, seed, kp, out, contribs, status, self_mass, query_base);
-  return cudaGetLastError();
+  if (self_mass || query_base)
+    return launch_sbh_variant<DIM, K, true>(t, q, nq, order, samples, seed, kp, out, contribs,
+                                            status, stream, sm_count, self_mass, query_base);
+  return launch_sbh_variant<DIM, K, false>(t, q, nq, order, samples, seed, kp, out, contribs,
+                                           status, stream, sm_count, self_mass, query_base);
 }
 
 }  // namespace
