@@ -47,6 +47,18 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 512 << 20
 
+# DRAM bytes (read + written) of one launch of each workload's main kernel at
+# its default size, from a single-pass ncu capture of the same bench command
+# (dram__bytes_read.sum + dram__bytes_write.sum, --clock-control none; the
+# commands and figures are in profiles/dram_traffic_full_launches.md).  Null in
+# the bench line when the query count or budget is overridden.
+DRAM_TRAFFIC = {
+    "sbh_wn": 5.38e9 + 369.71e6,
+    "bh_wn": 307.58e6 + 31.53e6,
+    "plain_small_bf": 1.85e6,
+    "plain_small_bh": 3.36e6,
+}
+
 WORKLOADS = {
     # name: (description, method, kernel, n points, n queries, tree kind, budget/beta)
     "sbh_wn": dict(desc="stochastic BH winding number, torus 1,048,576 pts, 4,194,304 queries, "
@@ -218,6 +230,13 @@ def dist_setup():
     return world, rank, local
 
 
+def dram_traffic(wl):
+    """DRAM bytes per launch of the workload's main kernel (ncu), or None."""
+    if wl.get("resized"):
+        return None
+    return DRAM_TRAFFIC.get(wl.get("name"))
+
+
 def run_ours(args, wl):
     import torch
 
@@ -360,7 +379,7 @@ def run_ours(args, wl):
                            f"{rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
                            f"{rates['sm_clock_mhz']:.0f} MHz; {mufu_per_pair} MUFU op(s) per pair",
             "kernel_ms": statistics.mean(kern_ms), "pairs_per_launch": pairs,
-            "pipe_rates": rates, "traffic": None,
+            "pipe_rates": rates, "traffic": dram_traffic(wl),
         }
     else:
         roofline = None
@@ -402,7 +421,7 @@ def run_ours(args, wl):
             "kernel_ms": statistics.mean(kern_ms),
             "algorithmic_bytes": alg_bytes,
             "bytes_definition": f"{bytes_per_eval} B per kernel evaluation (source or node record) + 16 B per query",
-            "traffic": None,
+            "traffic": dram_traffic(wl),
         },
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
@@ -1052,6 +1071,8 @@ def main():
     if args.workload in systems:
         ap.error("--impl reference runs the default workloads only")
     wl = dict(WORKLOADS[args.workload])
+    wl["name"] = args.workload
+    wl["resized"] = bool(args.nq or args.budget)
     if args.nq:
         wl["nq"] = args.nq
         wl["desc"] += f" [query count overridden: {args.nq}]"
