@@ -364,23 +364,23 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     const int pid = pbase + lane;
     V wd = A::zero();
     bool active = false;
-    int j = 0, S = 0, cur = 0;
-    int4 tcur = make_int4(0, 0, 0, 0);
+    int j = 0, cur = 0;
+    int4 tcur = make_int4(0, 0, 0, 0);  // topology of cur; .z = its point count
     float spi = 0.f, ev = 1.f, cb = 1.f;
     unsigned long long code = 0ull;  // the sampled point's path code
     int idx = 0, dcur = 1;           // the sampled point; depth of cur
     PathRng rng;
     if (pid < P) {
       j = pid / samples;
-      S = c0 + j;
+      const int S = c0 + j;
       const int4 tS = __ldg(t.nd_topo + S);
-      rng.begin(seed, (unsigned long long)qi, (uint32_t)pid);
+      rng.begin((uint32_t)pid);
       const uint32_t nS = (uint32_t)(tS.w - tS.z);
-      idx = tS.z + (int)rng.index(nS);
+      idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)qi);
       code = __ldg(t.pt_code + idx);
       spi = (float)nS;
       cur = S;
-      tcur = tS;
+      tcur = make_int4(tS.x, tS.y, tS.w - tS.z, 0);
       const float r0 = tS.y == 0 ? inf : far_field_ratio<DIM>(__ldg(t.nd_cm + S), q);
       cb = (1.f < r0) ? r0 : 1.f;
       active = tS.y != 0;
@@ -395,7 +395,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
         const float ffr = far_field_ratio<DIM>(cmc, q);
         const float ratio = rdiv(cb, ffr);
         const float tp = (1.f < ratio) ? 1.f : ratio;
-        const float u = rng.uniform();
+        const float u = rng.uniform(seed, (unsigned long long)qi);
         if (u > tp) {
           active = false;
         } else {
@@ -410,14 +410,14 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
             active = false;
           } else {
             cb = (cb < ffr) ? ffr : cb;
-            w = rdiv(spi, rmul(ev, (float)(unsigned)(tprev.w - tprev.z)));
-            if (prev == S) {
+            w = rdiv(spi, rmul(ev, (float)(unsigned)tprev.z));
+            if (prev == c0 + j) {
               wd = A::add(wd, A::scale(w, ws.diffS[j]));
               cnt += ws.ccS[j];
             } else {
               own = true;
             }
-            tcur = tnext;
+            tcur = make_int4(tnext.x, tnext.y, tnext.w - tnext.z, 0);
             if (tcur.y == 0) active = false;
           }
         }
