@@ -287,14 +287,24 @@ __device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 
 
 
 // Shared-memory scratch of one warp running the sampler (sbh_warp_words<V>
-// 4-byte words; V is the policy's value).
+// 4-byte words; V is the policy's value): the fixed-size arrays first, then
+// the three per-subdomain arrays, all found from the base and R so that the
+// warp keeps one pointer, not five.
 template <class V>
 struct SbhWarpSmem {
-  V* bhS;         // [R] BH term of each subdomain
-  V* diffS;       // [R] first-step difference of each subdomain
-  int* ccS;       // [R] contributions of that difference
-  V* pathv;       // [32] per-path corrections of the current round
-  int* ownlane;   // [32] lanes of the current expansion's owners, in order
+  float* base;
+  int R;
+  static constexpr int W = (int)(sizeof(V) / 4);
+  // [32] lanes of the current expansion's owners, in order
+  __device__ __forceinline__ int* ownlane() const { return reinterpret_cast<int*>(base); }
+  // [32] per-path corrections of the current round
+  __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 32); }
+  // [R] BH term of each subdomain
+  __device__ __forceinline__ V* bhS() const { return reinterpret_cast<V*>(base + 32 + 32 * W); }
+  // [R] first-step difference of each subdomain
+  __device__ __forceinline__ V* diffS() const { return bhS() + R; }
+  // [R] contributions of that difference
+  __device__ __forceinline__ int* ccS() const { return reinterpret_cast<int*>(diffS() + R); }
 };
 
 template <class V>
@@ -305,11 +315,8 @@ __host__ __device__ constexpr int sbh_warp_words(int R) {
 template <class V>
 __device__ __forceinline__ SbhWarpSmem<V> sbh_carve(float* base, int R) {
   SbhWarpSmem<V> w;
-  w.bhS = reinterpret_cast<V*>(base);
-  w.diffS = w.bhS + R;
-  w.ccS = reinterpret_cast<int*>(w.diffS + R);
-  w.pathv = reinterpret_cast<V*>(w.ccS + R);
-  w.ownlane = reinterpret_cast<int*>(w.pathv + 32);
+  w.base = base;
+  w.R = R;
   return w;
 }
 
@@ -347,11 +354,11 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     V kS = A::zero();
     if (own) kS = A::node(__ldg(t.nd_cm + c0 + j), __ldg(t.nd_agg + c0 + j), q, kp);
     int cc;
-    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, lane, ws.ownlane, cc);
+    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, lane, ws.ownlane(), cc);
     if (have) {
-      ws.bhS[j] = kS;
-      ws.diffS[j] = own ? A::sub(sumc, kS) : A::zero();
-      ws.ccS[j] = cc;
+      ws.bhS()[j] = kS;
+      ws.diffS()[j] = own ? A::sub(sumc, kS) : A::zero();
+      ws.ccS()[j] = cc;
     }
   }
   __syncwarp();
@@ -412,8 +419,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
             cb = (cb < ffr) ? ffr : cb;
             w = rdiv(spi, rmul(ev, (float)(unsigned)tprev.z));
             if (prev == c0 + j) {
-              wd = A::add(wd, A::scale(w, ws.diffS[j]));
-              cnt += ws.ccS[j];
+              wd = A::add(wd, A::scale(w, ws.diffS()[j]));
+              cnt += ws.ccS()[j];
             } else {
               own = true;
             }
@@ -423,14 +430,14 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
         }
       }
       int cc;
-      const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, ws.ownlane, cc);
+      const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, ws.ownlane(), cc);
       if (own) {
         const V kprev = A::node(__ldg(t.nd_cm + prev), __ldg(t.nd_agg + prev), q, kp);
         wd = A::add(wd, A::scale(w, A::sub(sumc, kprev)));
         cnt += cc;
       }
     }
-    ws.pathv[lane] = wd;
+    ws.pathv()[lane] = wd;
     __syncwarp();
     if (lane == 0) {
       const int m = min(32, P - pbase);
@@ -441,7 +448,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
           sub = A::zero();
           cur_sub = jj;
         }
-        sub = A::add(sub, ws.pathv[k]);
+        sub = A::add(sub, ws.pathv()[k]);
       }
     }
     __syncwarp();
@@ -457,7 +464,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       if (tS.y == 0) {
         bh = add_leaf_points<A>(t, tS, q, kp, bh);
       } else {
-        bh = A::add(bh, ws.bhS[j]);
+        bh = A::add(bh, ws.bhS()[j]);
       }
     }
     result = A::add(bh, mlcv);
