@@ -175,37 +175,32 @@ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint3
 
 // Random stream of one sampled path: key = seed, counter = (query, path, block).
 // Word 0 of block 0 picks the sample point; the remaining words, block after
-// block, are the Russian-roulette uniforms.  The key and the query index are
-// passed to every draw rather than kept in the state: they are the same for all
-// paths of a query, and the caller holds them anyway.
+// block, are the Russian-roulette uniforms.  The key, the query index and the
+// path index are passed to every draw rather than kept in the state (the
+// caller holds them anyway); the state is the current block's four words and
+// the number of words drawn (block = n / 4, word = n % 4).
 struct PathRng {
-  uint32_t path, block;
   Philox4 buf;
-  int word;
-  __device__ __forceinline__ void begin(uint32_t path_id) {
-    path = path_id;
-    block = 0;
-    word = 4;
-  }
-  __device__ __forceinline__ uint32_t next(unsigned long long seed, unsigned long long query) {
-    if (word == 4) {
-      buf = philox4x32_10((uint32_t)query, (uint32_t)(query >> 32), path, block, (uint32_t)seed,
+  uint32_t n;
+  __device__ __forceinline__ void begin() { n = 0; }
+  __device__ __forceinline__ uint32_t next(unsigned long long seed, unsigned long long query,
+                                           uint32_t path) {
+    const uint32_t word = n & 3u;
+    if (word == 0)
+      buf = philox4x32_10((uint32_t)query, (uint32_t)(query >> 32), path, n >> 2, (uint32_t)seed,
                           (uint32_t)(seed >> 32));
-      block++;
-      word = 0;
-    }
-    uint32_t r = word == 0 ? buf.x : word == 1 ? buf.y : word == 2 ? buf.z : buf.w;
-    word++;
-    return r;
+    n++;
+    return word == 0 ? buf.x : word == 1 ? buf.y : word == 2 ? buf.z : buf.w;
   }
-  // Uniform index in [0, n): multiply-shift of one 32-bit word.
-  __device__ __forceinline__ uint32_t index(uint32_t n, unsigned long long seed,
-                                            unsigned long long query) {
-    return (uint32_t)(((unsigned long long)next(seed, query) * n) >> 32);
+  // Uniform index in [0, m): multiply-shift of one 32-bit word.
+  __device__ __forceinline__ uint32_t index(uint32_t m, unsigned long long seed,
+                                            unsigned long long query, uint32_t path) {
+    return (uint32_t)(((unsigned long long)next(seed, query, path) * m) >> 32);
   }
   // Uniform float in [0, 1) on a 2^-24 grid.
-  __device__ __forceinline__ float uniform(unsigned long long seed, unsigned long long query) {
-    return (float)(next(seed, query) >> 8) * (1.0f / 16777216.0f);
+  __device__ __forceinline__ float uniform(unsigned long long seed, unsigned long long query,
+                                           uint32_t path) {
+    return (float)(next(seed, query, path) >> 8) * (1.0f / 16777216.0f);
   }
 };
 

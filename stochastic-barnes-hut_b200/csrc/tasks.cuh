@@ -370,20 +370,19 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
   for (int pbase = 0; pbase < P; pbase += 32) {
     const int pid = pbase + lane;
     V wd = A::zero();
-    bool active = false;
-    int j = 0, cur = 0;
+    bool active = false, first = false;  // first: the next step leaves the subdomain's root
+    int cur = 0;
     int4 tcur = make_int4(0, 0, 0, 0);  // topology of cur; .z = its point count
     float spi = 0.f, ev = 1.f, cb = 1.f;
     unsigned long long code = 0ull;  // the sampled point's path code
     int idx = 0, dcur = 1;           // the sampled point; depth of cur
     PathRng rng;
     if (pid < P) {
-      j = pid / samples;
-      const int S = c0 + j;
+      const int S = c0 + pid / samples;
       const int4 tS = __ldg(t.nd_topo + S);
-      rng.begin((uint32_t)pid);
+      rng.begin();
       const uint32_t nS = (uint32_t)(tS.w - tS.z);
-      idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)qi);
+      idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)qi, (uint32_t)pid);
       code = __ldg(t.pt_code + idx);
       spi = (float)nS;
       cur = S;
@@ -391,6 +390,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       const float r0 = tS.y == 0 ? inf : far_field_ratio<DIM>(__ldg(t.nd_cm + S), q);
       cb = (1.f < r0) ? r0 : 1.f;
       active = tS.y != 0;
+      first = true;
     }
     while (__any_sync(0xffffffffu, active)) {
       bool own = false;
@@ -402,7 +402,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
         const float ffr = far_field_ratio<DIM>(cmc, q);
         const float ratio = rdiv(cb, ffr);
         const float tp = (1.f < ratio) ? 1.f : ratio;
-        const float u = rng.uniform(seed, (unsigned long long)qi);
+        const float u = rng.uniform(seed, (unsigned long long)qi, (uint32_t)pid);
         if (u > tp) {
           active = false;
         } else {
@@ -418,9 +418,11 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
           } else {
             cb = (cb < ffr) ? ffr : cb;
             w = rdiv(spi, rmul(ev, (float)(unsigned)tprev.z));
-            if (prev == c0 + j) {
+            if (first) {
+              const int j = pid / samples;
               wd = A::add(wd, A::scale(w, ws.diffS()[j]));
               cnt += ws.ccS()[j];
+              first = false;
             } else {
               own = true;
             }
