@@ -289,7 +289,8 @@ __device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 
 // Shared-memory scratch of one warp running the sampler (sbh_warp_words<V>
 // 4-byte words; V is the policy's value): the fixed-size arrays first, then
 // the three per-subdomain arrays, all found from the base and R so that the
-// warp keeps one pointer, not five.
+// warp keeps one pointer, not five.  Lane 0's running sums of the paths live
+// here too, not in registers every lane would carry through the paths.
 template <class V>
 struct SbhWarpSmem {
   float* base;
@@ -299,8 +300,16 @@ struct SbhWarpSmem {
   __device__ __forceinline__ int* ownlane() const { return reinterpret_cast<int*>(base); }
   // [32] per-path corrections of the current round
   __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 32); }
+  // lane 0's fold of the paths: [0] the control-variate sum, [1] the current
+  // subdomain's sum of path corrections; then the current subdomain's index
+  __device__ __forceinline__ V* fold() const { return reinterpret_cast<V*>(base + 32 + 32 * W); }
+  __device__ __forceinline__ int* fold_sub() const {
+    return reinterpret_cast<int*>(base + 32 + 34 * W);
+  }
   // [R] BH term of each subdomain
-  __device__ __forceinline__ V* bhS() const { return reinterpret_cast<V*>(base + 32 + 32 * W); }
+  __device__ __forceinline__ V* bhS() const {
+    return reinterpret_cast<V*>(base + 33 + 34 * W);
+  }
   // [R] first-step difference of each subdomain
   __device__ __forceinline__ V* diffS() const { return bhS() + R; }
   // [R] contributions of that difference
@@ -309,7 +318,7 @@ struct SbhWarpSmem {
 
 template <class V>
 __host__ __device__ constexpr int sbh_warp_words(int R) {
-  return (int)(sizeof(V) / 4) * (2 * R + 32) + R + 32;
+  return (int)(sizeof(V) / 4) * (2 * R + 34) + R + 33;
 }
 
 template <class V>
@@ -365,14 +374,17 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
 
   // Phase B: sampled paths, 32 at a time, advanced step by step in lock step.
   const int P = R * samples;
-  V mlcv = A::zero(), sub = A::zero();
-  int cur_sub = -1;
+  if (lane == 0) {
+    ws.fold()[0] = A::zero();  // sum over subdomains of their mean path correction
+    ws.fold()[1] = A::zero();  // the current subdomain's sum of path corrections
+    *ws.fold_sub() = -1;
+  }
   for (int pbase = 0; pbase < P; pbase += 32) {
     const int pid = pbase + lane;
     V wd = A::zero();
     bool active = false, first = false;  // first: the next step leaves the subdomain's root
     int cur = 0;
-    int4 tcur = make_int4(0, 0, 0, 0);  // topology of cur; .z = its point count
+    int4 tcur = make_int4(0, 0, 0, 0);  // first child and child count of cur
     float spi = 0.f, ev = 1.f, cb = 1.f;
     unsigned long long code = 0ull;  // the sampled point's path code
     int idx = 0, dcur = 1;           // the sampled point; depth of cur
@@ -386,7 +398,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       code = __ldg(t.pt_code + idx);
       spi = (float)nS;
       cur = S;
-      tcur = make_int4(tS.x, tS.y, tS.w - tS.z, 0);
+      tcur = make_int4(tS.x, tS.y, 0, 0);
       const float r0 = tS.y == 0 ? inf : far_field_ratio<DIM>(__ldg(t.nd_cm + S), q);
       cb = (1.f < r0) ? r0 : 1.f;
       active = tS.y != 0;
@@ -417,7 +429,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
             active = false;
           } else {
             cb = (cb < ffr) ? ffr : cb;
-            w = rdiv(spi, rmul(ev, (float)(unsigned)tprev.z));
+            const int4 tp4 = __ldg(t.nd_topo + prev);  // prev's point range
+            w = rdiv(spi, rmul(ev, (float)(unsigned)(tp4.w - tp4.z)));
             if (first) {
               const int j = pid / samples;
               wd = A::add(wd, A::scale(w, ws.diffS()[j]));
@@ -426,7 +439,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
             } else {
               own = true;
             }
-            tcur = make_int4(tnext.x, tnext.y, tnext.w - tnext.z, 0);
+            tcur = make_int4(tnext.x, tnext.y, 0, 0);
             if (tcur.y == 0) active = false;
           }
         }
@@ -442,6 +455,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     ws.pathv()[lane] = wd;
     __syncwarp();
     if (lane == 0) {
+      V mlcv = ws.fold()[0], sub = ws.fold()[1];
+      int cur_sub = *ws.fold_sub();
       const int m = min(32, P - pbase);
       for (int k = 0; k < m; k++) {
         const int jj = (pbase + k) / samples;
@@ -452,6 +467,9 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
         }
         sub = A::add(sub, ws.pathv()[k]);
       }
+      ws.fold()[0] = mlcv;
+      ws.fold()[1] = sub;
+      *ws.fold_sub() = cur_sub;
     }
     __syncwarp();
   }
@@ -459,7 +477,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if (lane == 0) {
-    if (cur_sub >= 0) mlcv = A::add(mlcv, A::div(sub, (float)samples));
+    V mlcv = ws.fold()[0];
+    if (*ws.fold_sub() >= 0) mlcv = A::add(mlcv, A::div(ws.fold()[1], (float)samples));
     V bh = A::zero();
     for (int j = 0; j < R; j++) {
       const int4 tS = __ldg(t.nd_topo + c0 + j);
