@@ -177,30 +177,39 @@ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint3
 // Word 0 of block 0 picks the sample point; the remaining words, block after
 // block, are the Russian-roulette uniforms.  The key, the query index and the
 // path index are passed to every draw rather than kept in the state (the
-// caller holds them anyway); the state is the current block's four words and
-// the number of words drawn (block = n / 4, word = n % 4).
+// caller holds them anyway); a block's words 1-3 wait in the caller's shared
+// memory (`buf[32 * w]`, one column per lane), so the state in registers is
+// only the number of words drawn (block = n / 4, word = n % 4).
 struct PathRng {
-  Philox4 buf;
   uint32_t n;
   __device__ __forceinline__ void begin() { n = 0; }
   __device__ __forceinline__ uint32_t next(unsigned long long seed, unsigned long long query,
-                                           uint32_t path) {
+                                           uint32_t path, uint32_t* buf) {
     const uint32_t word = n & 3u;
-    if (word == 0)
-      buf = philox4x32_10((uint32_t)query, (uint32_t)(query >> 32), path, n >> 2, (uint32_t)seed,
-                          (uint32_t)(seed >> 32));
+    uint32_t r;
+    if (word == 0) {
+      const Philox4 b = philox4x32_10((uint32_t)query, (uint32_t)(query >> 32), path, n >> 2,
+                                      (uint32_t)seed, (uint32_t)(seed >> 32));
+      buf[32] = b.y;
+      buf[64] = b.z;
+      buf[96] = b.w;
+      r = b.x;
+    } else {
+      r = buf[32 * word];
+    }
     n++;
-    return word == 0 ? buf.x : word == 1 ? buf.y : word == 2 ? buf.z : buf.w;
+    return r;
   }
   // Uniform index in [0, m): multiply-shift of one 32-bit word.
   __device__ __forceinline__ uint32_t index(uint32_t m, unsigned long long seed,
-                                            unsigned long long query, uint32_t path) {
-    return (uint32_t)(((unsigned long long)next(seed, query, path) * m) >> 32);
+                                            unsigned long long query, uint32_t path,
+                                            uint32_t* buf) {
+    return (uint32_t)(((unsigned long long)next(seed, query, path, buf) * m) >> 32);
   }
   // Uniform float in [0, 1) on a 2^-24 grid.
   __device__ __forceinline__ float uniform(unsigned long long seed, unsigned long long query,
-                                           uint32_t path) {
-    return (float)(next(seed, query, path) >> 8) * (1.0f / 16777216.0f);
+                                           uint32_t path, uint32_t* buf) {
+    return (float)(next(seed, query, path, buf) >> 8) * (1.0f / 16777216.0f);
   }
 };
 

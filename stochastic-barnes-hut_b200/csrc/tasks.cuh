@@ -298,17 +298,21 @@ struct SbhWarpSmem {
   static constexpr int W = (int)(sizeof(V) / 4);
   // [32] lanes of the current expansion's owners, in order
   __device__ __forceinline__ int* ownlane() const { return reinterpret_cast<int*>(base); }
+  // [4][32] the paths' pending random words (PathRng; word w of lane l at [w][l])
+  __device__ __forceinline__ uint32_t* rngbuf() const {
+    return reinterpret_cast<uint32_t*>(base + 32);
+  }
   // [32] per-path corrections of the current round
-  __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 32); }
+  __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 160); }
   // lane 0's fold of the paths: [0] the control-variate sum, [1] the current
   // subdomain's sum of path corrections; then the current subdomain's index
-  __device__ __forceinline__ V* fold() const { return reinterpret_cast<V*>(base + 32 + 32 * W); }
+  __device__ __forceinline__ V* fold() const { return reinterpret_cast<V*>(base + 160 + 32 * W); }
   __device__ __forceinline__ int* fold_sub() const {
-    return reinterpret_cast<int*>(base + 32 + 34 * W);
+    return reinterpret_cast<int*>(base + 160 + 34 * W);
   }
   // [R] BH term of each subdomain
   __device__ __forceinline__ V* bhS() const {
-    return reinterpret_cast<V*>(base + 33 + 34 * W);
+    return reinterpret_cast<V*>(base + 161 + 34 * W);
   }
   // [R] first-step difference of each subdomain
   __device__ __forceinline__ V* diffS() const { return bhS() + R; }
@@ -318,7 +322,7 @@ struct SbhWarpSmem {
 
 template <class V>
 __host__ __device__ constexpr int sbh_warp_words(int R) {
-  return (int)(sizeof(V) / 4) * (2 * R + 34) + R + 33;
+  return (int)(sizeof(V) / 4) * (2 * R + 34) + R + 161;
 }
 
 template <class V>
@@ -394,7 +398,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       const int4 tS = __ldg(t.nd_topo + S);
       rng.begin();
       const uint32_t nS = (uint32_t)(tS.w - tS.z);
-      idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)qi, (uint32_t)pid);
+      idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)qi, (uint32_t)pid,
+                                  ws.rngbuf() + lane);
       code = __ldg(t.pt_code + idx);
       spi = (float)nS;
       cur = S;
@@ -414,7 +419,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
         const float ffr = far_field_ratio<DIM>(cmc, q);
         const float ratio = rdiv(cb, ffr);
         const float tp = (1.f < ratio) ? 1.f : ratio;
-        const float u = rng.uniform(seed, (unsigned long long)qi, (uint32_t)pid);
+        const float u =
+            rng.uniform(seed, (unsigned long long)qi, (uint32_t)pid, ws.rngbuf() + lane);
         if (u > tp) {
           active = false;
         } else {
