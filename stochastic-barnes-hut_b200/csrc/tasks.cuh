@@ -333,6 +333,15 @@ __device__ __forceinline__ SbhWarpSmem<V> sbh_carve(float* base, int R) {
   return w;
 }
 
+// Weight of a path's step out of node v: (points of the subdomain) / (path
+// probability so far x points of v), rounded as the reference rounds it
+// (include/tree_sampler.h:102-103, sample_prob_inv / (event_prob *
+// prev_node->numContainedPoints())).
+__device__ __forceinline__ float path_weight(const DevTree& t, int v, float spi, float ev) {
+  const int4 tv = __ldg(t.nd_topo + v);
+  return rdiv(spi, rmul(ev, (float)(unsigned)(tv.w - tv.z)));
+}
+
 // The whole estimator for one query, one warp: see sampler.cu for the method.
 // qi is the query's index in its request (it keys the Philox streams).  The
 // result and its contribution count are returned on lane 0.  Sums follow the
@@ -413,7 +422,6 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       bool own = false;
       int prev = 0;
       int4 tprev = make_int4(0, 0, 0, 0);
-      float w = 0.f;
       if (active) {
         const float4 cmc = __ldg(t.nd_cm + cur);
         const float ffr = far_field_ratio<DIM>(cmc, q);
@@ -435,9 +443,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
             active = false;
           } else {
             cb = (cb < ffr) ? ffr : cb;
-            const int4 tp4 = __ldg(t.nd_topo + prev);  // prev's point range
-            w = rdiv(spi, rmul(ev, (float)(unsigned)(tp4.w - tp4.z)));
             if (first) {
+              const float w = path_weight(t, prev, spi, ev);
               const int j = pid / samples;
               wd = A::add(wd, A::scale(w, ws.diffS()[j]));
               cnt += ws.ccS()[j];
@@ -453,6 +460,9 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       int cc;
       const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, ws.ownlane(), cc);
       if (own) {
+        // The step's weight is formed here, after the expansion, so that it is
+        // not carried through it.
+        const float w = path_weight(t, prev, spi, ev);
         const V kprev = A::node(__ldg(t.nd_cm + prev), __ldg(t.nd_agg + prev), q, kp);
         wd = A::add(wd, A::scale(w, A::sub(sumc, kprev)));
         cnt += cc;
