@@ -245,7 +245,8 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
 // would return nullptr.
 template <int DIM>
 __device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 tv, int dv,
-                                                  unsigned long long code, int idx, int4& tout,
+                                                  unsigned long long code, const int* idx_slot,
+                                                  int4& tout,
                                                   int& dout) {
   const bool coded = (code >> 63) == 0ull;
   const unsigned cell_mask = (1u << t.code_bits) - 1u;
@@ -254,7 +255,7 @@ __device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 
     if (coded && dv < t.code_levels) {
       cell = (int)((code >> (t.code_bits * dv)) & cell_mask);
     } else {
-      const float4 sp = __ldg(t.pt_pm + idx);
+      const float4 sp = __ldg(t.pt_pm + *idx_slot);
       const float3 p = make_float3(sp.x, sp.y, sp.z);
       const float4 lo = __ldg(t.nd_bmin + v), hi = __ldg(t.nd_bmax + v);
       if (!aabb_contains<DIM>(lo, hi, p)) return -1;
@@ -302,17 +303,21 @@ struct SbhWarpSmem {
   __device__ __forceinline__ uint32_t* rngbuf() const {
     return reinterpret_cast<uint32_t*>(base + 32);
   }
+  // [32] each path's sampled point and [32] its subdomain's point count (as a
+  // float): read once per step, so they wait here rather than in registers
+  __device__ __forceinline__ int* path_point() const { return reinterpret_cast<int*>(base + 160); }
+  __device__ __forceinline__ float* path_spi() const { return base + 192; }
   // [32] per-path corrections of the current round
-  __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 160); }
+  __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 224); }
   // lane 0's fold of the paths: [0] the control-variate sum, [1] the current
   // subdomain's sum of path corrections; then the current subdomain's index
-  __device__ __forceinline__ V* fold() const { return reinterpret_cast<V*>(base + 160 + 32 * W); }
+  __device__ __forceinline__ V* fold() const { return reinterpret_cast<V*>(base + 224 + 32 * W); }
   __device__ __forceinline__ int* fold_sub() const {
-    return reinterpret_cast<int*>(base + 160 + 34 * W);
+    return reinterpret_cast<int*>(base + 224 + 34 * W);
   }
   // [R] BH term of each subdomain
   __device__ __forceinline__ V* bhS() const {
-    return reinterpret_cast<V*>(base + 161 + 34 * W);
+    return reinterpret_cast<V*>(base + 225 + 34 * W);
   }
   // [R] first-step difference of each subdomain
   __device__ __forceinline__ V* diffS() const { return bhS() + R; }
@@ -322,7 +327,7 @@ struct SbhWarpSmem {
 
 template <class V>
 __host__ __device__ constexpr int sbh_warp_words(int R) {
-  return (int)(sizeof(V) / 4) * (2 * R + 34) + R + 161;
+  return (int)(sizeof(V) / 4) * (2 * R + 34) + R + 225;
 }
 
 template <class V>
@@ -398,19 +403,20 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     bool active = false, first = false;  // first: the next step leaves the subdomain's root
     int cur = 0;
     int4 tcur = make_int4(0, 0, 0, 0);  // first child and child count of cur
-    float spi = 0.f, ev = 1.f, cb = 1.f;
+    float ev = 1.f, cb = 1.f;
     unsigned long long code = 0ull;  // the sampled point's path code
-    int idx = 0, dcur = 1;           // the sampled point; depth of cur
+    int dcur = 1;                    // depth of cur
     PathRng rng;
     if (pid < P) {
       const int S = c0 + pid / samples;
       const int4 tS = __ldg(t.nd_topo + S);
       rng.begin();
       const uint32_t nS = (uint32_t)(tS.w - tS.z);
-      idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)qi, (uint32_t)pid,
-                                  ws.rngbuf() + lane);
+      const int idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)qi, (uint32_t)pid,
+                                            ws.rngbuf() + lane);
       code = __ldg(t.pt_code + idx);
-      spi = (float)nS;
+      ws.path_point()[lane] = idx;
+      ws.path_spi()[lane] = (float)nS;
       cur = S;
       tcur = make_int4(tS.x, tS.y, 0, 0);
       const float r0 = tS.y == 0 ? inf : far_field_ratio<DIM>(__ldg(t.nd_cm + S), q);
@@ -436,7 +442,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
           prev = cur;
           tprev = tcur;
           int4 tnext;
-          cur = contained_in_child<DIM>(t, prev, tprev, dcur, code, idx, tnext, dcur);
+          cur = contained_in_child<DIM>(t, prev, tprev, dcur, code, ws.path_point() + lane, tnext,
+                                        dcur);
           if (cur < 0) {
             report_status(status, kStatusNullChild);
             wd = A::nan();
@@ -444,7 +451,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
           } else {
             cb = (cb < ffr) ? ffr : cb;
             if (first) {
-              const float w = path_weight(t, prev, spi, ev);
+              const float w = path_weight(t, prev, ws.path_spi()[lane], ev);
               const int j = pid / samples;
               wd = A::add(wd, A::scale(w, ws.diffS()[j]));
               cnt += ws.ccS()[j];
@@ -462,7 +469,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       if (own) {
         // The step's weight is formed here, after the expansion, so that it is
         // not carried through it.
-        const float w = path_weight(t, prev, spi, ev);
+        const float w = path_weight(t, prev, ws.path_spi()[lane], ev);
         const V kprev = A::node(__ldg(t.nd_cm + prev), __ldg(t.nd_agg + prev), q, kp);
         wd = A::add(wd, A::scale(w, A::sub(sumc, kprev)));
         cnt += cc;
