@@ -230,9 +230,11 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
   return acc;
 }
 
-// containedInChild(VectorNd p) (include/tree3d.h:172-183) for sampled point
-// `idx`: the child of v (at depth dv) whose cell holds the point, skipping
-// single-child chains; *dout receives the depth of the node returned.
+// containedInChild(VectorNd p) (include/tree3d.h:172-183) for a path's sampled
+// point, whose index (`*idx_slot`) and path code (`code_slot[0]` low word,
+// `code_slot[32]` high word) wait in shared memory: the child of v (at depth
+// dv) whose cell holds the point, skipping single-child chains; *dout receives
+// the depth of the node returned.
 //
 // The cell comes from the point's path code when it holds one: the cells the
 // build assigned the point at every level (upload computes them from the
@@ -245,9 +247,10 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
 // would return nullptr.
 template <int DIM>
 __device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 tv, int dv,
-                                                  unsigned long long code, const int* idx_slot,
-                                                  int4& tout,
-                                                  int& dout) {
+                                                  const uint32_t* code_slot, const int* idx_slot,
+                                                  int4& tout, int& dout) {
+  const unsigned long long code =
+      (unsigned long long)code_slot[0] | ((unsigned long long)code_slot[32] << 32);
   const bool coded = (code >> 63) == 0ull;
   const unsigned cell_mask = (1u << t.code_bits) - 1u;
   for (int guard = 0; guard <= t.depth + 1; guard++) {
@@ -307,17 +310,21 @@ struct SbhWarpSmem {
   // float): read once per step, so they wait here rather than in registers
   __device__ __forceinline__ int* path_point() const { return reinterpret_cast<int*>(base + 160); }
   __device__ __forceinline__ float* path_spi() const { return base + 192; }
+  // [32] each path's sampled point's path code, as two words (low [32], high [32])
+  __device__ __forceinline__ uint32_t* path_code() const {
+    return reinterpret_cast<uint32_t*>(base + 224);
+  }
   // [32] per-path corrections of the current round
-  __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 224); }
+  __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 288); }
   // lane 0's fold of the paths: [0] the control-variate sum, [1] the current
   // subdomain's sum of path corrections; then the current subdomain's index
-  __device__ __forceinline__ V* fold() const { return reinterpret_cast<V*>(base + 224 + 32 * W); }
+  __device__ __forceinline__ V* fold() const { return reinterpret_cast<V*>(base + 288 + 32 * W); }
   __device__ __forceinline__ int* fold_sub() const {
-    return reinterpret_cast<int*>(base + 224 + 34 * W);
+    return reinterpret_cast<int*>(base + 288 + 34 * W);
   }
   // [R] BH term of each subdomain
   __device__ __forceinline__ V* bhS() const {
-    return reinterpret_cast<V*>(base + 225 + 34 * W);
+    return reinterpret_cast<V*>(base + 289 + 34 * W);
   }
   // [R] first-step difference of each subdomain
   __device__ __forceinline__ V* diffS() const { return bhS() + R; }
@@ -327,7 +334,7 @@ struct SbhWarpSmem {
 
 template <class V>
 __host__ __device__ constexpr int sbh_warp_words(int R) {
-  return (int)(sizeof(V) / 4) * (2 * R + 34) + R + 225;
+  return (int)(sizeof(V) / 4) * (2 * R + 34) + R + 289;
 }
 
 template <class V>
@@ -404,7 +411,6 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     int cur = 0;
     int4 tcur = make_int4(0, 0, 0, 0);  // first child and child count of cur
     float ev = 1.f, cb = 1.f;
-    unsigned long long code = 0ull;  // the sampled point's path code
     int dcur = 1;                    // depth of cur
     PathRng rng;
     if (pid < P) {
@@ -414,7 +420,9 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       const uint32_t nS = (uint32_t)(tS.w - tS.z);
       const int idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)qi, (uint32_t)pid,
                                             ws.rngbuf() + lane);
-      code = __ldg(t.pt_code + idx);
+      const unsigned long long code = __ldg(t.pt_code + idx);
+      ws.path_code()[lane] = (uint32_t)code;
+      ws.path_code()[32 + lane] = (uint32_t)(code >> 32);
       ws.path_point()[lane] = idx;
       ws.path_spi()[lane] = (float)nS;
       cur = S;
@@ -442,8 +450,8 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
           prev = cur;
           tprev = tcur;
           int4 tnext;
-          cur = contained_in_child<DIM>(t, prev, tprev, dcur, code, ws.path_point() + lane, tnext,
-                                        dcur);
+          cur = contained_in_child<DIM>(t, prev, tprev, dcur, ws.path_code() + lane,
+                                        ws.path_point() + lane, tnext, dcur);
           if (cur < 0) {
             report_status(status, kStatusNullChild);
             wd = A::nan();
