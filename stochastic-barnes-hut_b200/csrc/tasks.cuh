@@ -328,7 +328,7 @@ struct SbhWarpSmem {
   }
   // [R] first-step difference of each subdomain
   __device__ __forceinline__ V* diffS() const { return bhS() + R; }
-  // [R] contributions of that difference
+  // [R] contributions of that difference (-1: a leaf subdomain)
   __device__ __forceinline__ int* ccS() const { return reinterpret_cast<int*>(diffS() + R); }
 };
 
@@ -392,7 +392,7 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
     if (have) {
       ws.bhS()[j] = kS;
       ws.diffS()[j] = own ? A::sub(sumc, kS) : A::zero();
-      ws.ccS()[j] = cc;
+      ws.ccS()[j] = own ? cc : -1;  // -1: a leaf subdomain (no path leaves it)
     }
   }
   __syncwarp();
@@ -484,23 +484,46 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
       }
     }
     ws.pathv()[lane] = wd;
+    // Fold the round's paths into the estimate, in path order: each run of
+    // consecutive paths of one subdomain (a group) is summed left to right by
+    // its first lane -- the first group continuing the previous round's last
+    // one from its carried partial sum -- and the completed groups' means are
+    // added to the running sum in group order by lane 0.  The same additions
+    // in the same order as one lane walking every path.
+    const V carry = ws.fold()[1];
+    const int carry_sub = *ws.fold_sub();
     __syncwarp();
-    if (lane == 0) {
-      V mlcv = ws.fold()[0], sub = ws.fold()[1];
-      int cur_sub = *ws.fold_sub();
-      const int m = min(32, P - pbase);
-      for (int k = 0; k < m; k++) {
-        const int jj = (pbase + k) / samples;
-        if (jj != cur_sub) {
-          if (cur_sub >= 0) mlcv = A::add(mlcv, A::div(sub, (float)samples));
-          sub = A::zero();
-          cur_sub = jj;
+    {
+      const unsigned full = 0xffffffffu;
+      const int m = min(32, P - pbase);  // paths in this round
+      const int jl = lane < m ? (pbase + lane) / samples : -1;
+      const int jprev = __shfl_up_sync(full, jl, 1);
+      const bool head = lane < m && (lane == 0 || jprev != jl);
+      const unsigned heads = __ballot_sync(full, head);
+      bool complete = false;
+      if (head) {
+        const unsigned later = lane == 31 ? 0u : heads & ~((2u << lane) - 1u);
+        const int end = later ? __ffs(later) - 1 : m;
+        V sum = (lane == 0 && jl == carry_sub) ? carry : A::zero();
+        for (int k = lane; k < end; k++) sum = A::add(sum, ws.pathv()[k]);
+        complete = end < m || pbase + m == P || (pbase + m) / samples != jl;
+        if (complete) ws.pathv()[lane] = A::div(sum, (float)samples);  // its own slot, read
+        if (later == 0) {                                                // the round's last group
+          if (complete) {
+            *ws.fold_sub() = -1;
+          } else {
+            ws.fold()[1] = sum;
+            *ws.fold_sub() = jl;
+          }
         }
-        sub = A::add(sub, ws.pathv()[k]);
       }
-      ws.fold()[0] = mlcv;
-      ws.fold()[1] = sub;
-      *ws.fold_sub() = cur_sub;
+      const unsigned done = __ballot_sync(full, head && complete);
+      __syncwarp();
+      if (lane == 0) {
+        V mlcv = ws.fold()[0];
+        for (unsigned d = done; d != 0u; d &= d - 1u) mlcv = A::add(mlcv, ws.pathv()[__ffs(d) - 1]);
+        ws.fold()[0] = mlcv;
+      }
     }
     __syncwarp();
   }
@@ -508,13 +531,11 @@ __device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long 
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if (lane == 0) {
-    V mlcv = ws.fold()[0];
-    if (*ws.fold_sub() >= 0) mlcv = A::add(mlcv, A::div(ws.fold()[1], (float)samples));
+    const V mlcv = ws.fold()[0];  // every group completed in the last round
     V bh = A::zero();
     for (int j = 0; j < R; j++) {
-      const int4 tS = __ldg(t.nd_topo + c0 + j);
-      if (tS.y == 0) {
-        bh = add_leaf_points<A>(t, tS, q, kp, bh);
+      if (ws.ccS()[j] < 0) {  // a leaf subdomain: its points, in order
+        bh = add_leaf_points<A>(t, __ldg(t.nd_topo + c0 + j), q, kp, bh);
       } else {
         bh = A::add(bh, ws.bhS()[j]);
       }
