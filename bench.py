@@ -53,7 +53,7 @@ L2_FLUSH_BYTES = 512 << 20
 # commands and figures are in profiles/dram_traffic_full_launches.md).  Null in
 # the bench line when the query count or budget is overridden.
 DRAM_TRAFFIC = {
-    "sbh_wn": 4.26e9 + 160.67e6,
+    "sbh_wn": 4.39e9 + 208.95e6,
     "bh_wn": 307.58e6 + 31.53e6,
     "plain_small_bf": 1.85e6,
     "plain_small_bh": 3.36e6,
