@@ -29,7 +29,9 @@
 //     the warp expands all nodes the step needs together.  Each path draws its
 //     own Philox4x32-10 stream keyed by (seed, query index, path index), so
 //     results do not depend on launch shape, batching or query order.
-//   * Lane 0 adds the per-path corrections and BH terms in the reference's order.
+//   * The per-path corrections and BH terms are added in the reference's order:
+//     each subdomain's paths left to right by the first lane holding one of
+//     them, the subdomains' means and the BH terms by lane 0.
 // With identical random decisions the estimator takes exactly the reference
 // CPU estimator's paths and terms, each term rounded as the reference rounds it
 // (IEEE single rounding, see device_common.cuh); only each node's children sum
