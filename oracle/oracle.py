@@ -76,12 +76,34 @@ def oracle_lib() -> ctypes.CDLL:
         lib.orc_bh_grad.argtypes = [_P, ctypes.c_int, _P, _I64, _F, _F, _F, _P, _P, _P]
         lib.orc_sbh_grad.argtypes = [_P, ctypes.c_int, _P, _I64, ctypes.c_int, ctypes.c_uint64,
                                      _F, _F, _P, _P, _P]
+        lib.orc_sbh_deepest.argtypes = [_P, ctypes.c_int, _P, _I64, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_uint64, _P, _F, _P]
+        lib.orc_sbh_grad_rng.argtypes = [_P, ctypes.c_int, _P, _I64, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_uint64, _P, _F, _F, _P, _P, _P]
         lib.orc_brute_force_grad_f64.argtypes = [_P, _P, _I64, ctypes.c_int, ctypes.c_int, _F, _F,
                                                  _P, _I64, _P, _P]
         lib.orc_philox4x32_10.argtypes = [_P, _P, _P]
         lib.orc_mt19937_stream.argtypes = [ctypes.c_uint32, _I64, _P, _P]
         lib._typed = True
     return lib
+
+
+_gpu_lib = None
+
+
+def gpu_lib() -> ctypes.CDLL:
+    """libsbh_bf64.so: the FP64 GPU brute force."""
+    global _gpu_lib
+    if _gpu_lib is None:
+        path = os.path.join(HERE, "libsbh_bf64.so")
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is not built; run `make -C {HERE}`")
+        lib = ctypes.CDLL(path)
+        lib.orc_gpu_brute_force_f64.restype = ctypes.c_int
+        lib.orc_gpu_brute_force_f64.argtypes = [_P, _P, _P, _I64, ctypes.c_int, ctypes.c_int, _F,
+                                                _F, _P, _I64, ctypes.c_int, _P]
+        _gpu_lib = lib
+    return _gpu_lib
 
 
 def ref_available() -> bool:
@@ -99,6 +121,7 @@ def ref_lib() -> ctypes.CDLL:
         lib.ref_tree_num_points.restype = _I64
         lib.ref_tree_num_points.argtypes = [_P]
         lib.ref_tree_branch.argtypes = [_P]
+        lib.ref_tree_root_children.argtypes = [_P]
         lib.ref_tree_dump_nodes.argtypes = [_P] * 12
         lib.ref_tree_dump_points.argtypes = [_P] * 5
         lib.ref_bh.argtypes = [_P, ctypes.c_int, _P, _I64, _F, _F, _P, _P, _P]
@@ -226,6 +249,18 @@ class OracleTree(_TreeBase):
         return (out, cnt, sc) if return_scale else (out, cnt)
 
 
+    def sbh_deepest(self, kernel, queries, samples, rng=RNG_PHILOX, seed=0, mt_seeds=None,
+                    eps=1e-3):
+        """Per query, the depth of the deepest node the sampler's paths reach
+        (the paths of sbh() with the same stream)."""
+        q = _f32(queries, (-1, self.dim))
+        nq = q.shape[0]
+        deep = np.zeros(nq, np.int32)
+        ms = None if mt_seeds is None else np.ascontiguousarray(mt_seeds, np.uint32)
+        self.lib.orc_sbh_deepest(self._h, kernel, _ptr(q), nq, samples, rng, seed, _ptr(ms), eps,
+                                 _ptr(deep))
+        return deep
+
     def bh_grad(self, kernel, queries, beta, alpha=1.0, eps=1e-3):
         """Barnes-Hut value and gradient in FP64 over the reference's node set:
         (val[nq], grad[nq, dim], counts)."""
@@ -238,16 +273,19 @@ class OracleTree(_TreeBase):
                              float(np.float32(alpha)), _ptr(val), _ptr(grad), _ptr(cnt))
         return val, grad, cnt
 
-    def sbh_grad(self, kernel, queries, samples, seed=0, alpha=1.0, eps=1e-3):
-        """Stochastic estimator value and gradient on the Philox paths of sbh():
-        (val[nq], grad[nq, dim], counts)."""
+    def sbh_grad(self, kernel, queries, samples, seed=0, alpha=1.0, eps=1e-3, rng=RNG_PHILOX,
+                 mt_seeds=None):
+        """Stochastic estimator value and gradient on the paths of sbh() with the
+        same random stream (Philox keyed by seed, or the reference's mt19937
+        seeded per query from mt_seeds): (val[nq], grad[nq, dim], counts)."""
         q = _f32(queries, (-1, self.dim))
         nq = q.shape[0]
         val = np.zeros(nq, np.float64)
         grad = np.zeros((nq, self.dim), np.float64)
         cnt = np.zeros(nq, np.int32)
-        self.lib.orc_sbh_grad(self._h, kernel, _ptr(q), nq, samples, seed, eps,
-                              float(np.float32(alpha)), _ptr(val), _ptr(grad), _ptr(cnt))
+        ms = None if mt_seeds is None else np.ascontiguousarray(mt_seeds, np.uint32)
+        self.lib.orc_sbh_grad_rng(self._h, kernel, _ptr(q), nq, samples, rng, seed, _ptr(ms), eps,
+                                  float(np.float32(alpha)), _ptr(val), _ptr(grad), _ptr(cnt))
         return val, grad, cnt
 
 
@@ -272,6 +310,7 @@ class RefTree(_TreeBase):
             raise ValueError("unsupported reference tree type")
         self.num_nodes = self.lib.ref_tree_num_nodes(self._h)
         self.branch = self.lib.ref_tree_branch(self._h)
+        self.root_children = self.lib.ref_tree_root_children(self._h)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -335,6 +374,26 @@ def brute_force_f64(points, normals, masses, kernel, queries, alpha=1.0, eps=1e-
     fn = lib.orc_brute_force_abs_f64 if abs_sum else lib.orc_brute_force_f64
     fn(_ptr(pts), _ptr(nrm), _ptr(m), n, dim, kernel, float(np.float32(alpha)),
        float(np.float32(eps)), _ptr(q), q.shape[0], _ptr(out))
+    return out
+
+
+def gpu_brute_force_f64(points, normals, masses, kernel, queries, alpha=1.0, eps=1e-3,
+                        abs_sum=False):
+    """brute_force_f64 on the GPU (libsbh_bf64.so): every term in FP64 from the
+    float inputs, summed over every source, for checks at benchmark scale."""
+    lib = gpu_lib()
+    pts = _f32(points)
+    dim = pts.shape[1]
+    n = pts.shape[0]
+    nrm = _f32(normals, (n, dim))
+    m = _f32(masses, (n,))
+    q = _f32(queries, (-1, dim))
+    out = np.zeros(q.shape[0], np.float64)
+    rc = lib.orc_gpu_brute_force_f64(_ptr(pts), _ptr(nrm), _ptr(m), n, dim, kernel,
+                                     float(np.float32(alpha)), float(np.float32(eps)), _ptr(q),
+                                     q.shape[0], int(abs_sum), _ptr(out))
+    if rc != 0:
+        raise RuntimeError(f"orc_gpu_brute_force_f64 failed with CUDA error {rc}")
     return out
 
 

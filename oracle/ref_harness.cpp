@@ -126,6 +126,7 @@ struct RefTreeBase {
   virtual int branch() const = 0;
   virtual int64_t num_nodes() const = 0;
   virtual int64_t num_points() const = 0;
+  virtual int root_children() const = 0;
   virtual void dump_nodes(int64_t*, int64_t*, int64_t*, int32_t*, int32_t*, uint8_t*, int64_t*,
                           float*, float*, float*, float*) const = 0;
   virtual void dump_points(float*, float*, float*, float*) const = 0;
@@ -160,6 +161,10 @@ struct RefTree : RefTreeBase {
   int branch() const override { return (int)Node::BranchFactor; }
   int64_t num_nodes() const override { return (int64_t)t->tree->node_vector().size(); }
   int64_t num_points() const override { return (int64_t)t->leaf_data.size(); }
+  int root_children() const override {
+    const auto& nodes = t->tree->node_vector();
+    return nodes.empty() ? 0 : (int)nodes[0].num_children();
+  }
 
   void dump_nodes(int64_t* start, int64_t* end, int64_t* parent, int32_t* depth, int32_t* nch,
                   uint8_t* leaf, int64_t* child, float* bmin, float* bmax, float* diam,
@@ -307,6 +312,9 @@ REF_API void ref_tree_destroy(void* h) { delete static_cast<RefTreeBase*>(h); }
 REF_API int64_t ref_tree_num_nodes(void* h) { return static_cast<RefTreeBase*>(h)->num_nodes(); }
 REF_API int64_t ref_tree_num_points(void* h) { return static_cast<RefTreeBase*>(h)->num_points(); }
 REF_API int ref_tree_branch(void* h) { return static_cast<RefTreeBase*>(h)->branch(); }
+REF_API int ref_tree_root_children(void* h) {
+  return static_cast<RefTreeBase*>(h)->root_children();
+}
 REF_API void ref_tree_dump_nodes(void* h, int64_t* start, int64_t* end, int64_t* parent, int32_t* depth,
                          int32_t* nch, uint8_t* leaf, int64_t* child, float* bmin, float* bmax,
                          float* diam, float* agg) {

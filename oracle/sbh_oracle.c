@@ -652,6 +652,7 @@ typedef struct {
   int32_t* counts;
   uint64_t* hashes;
   double* scales;
+  int32_t* deepest; /* sampler: depth of the deepest node any path of the query reached */
 } eval_ctx;
 
 static void bh_body(void* vc, int64_t i) {
@@ -665,7 +666,7 @@ static void bh_body(void* vc, int64_t i) {
 
 void orc_bh(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta, float eps,
             float* out, int32_t* counts, uint64_t* hashes) {
-  eval_ctx c = {t, kernel, 0, 0, 0, q, nq, beta, eps, 0, NULL, out, counts, hashes, NULL};
+  eval_ctx c = {t, kernel, 0, 0, 0, q, nq, beta, eps, 0, NULL, out, counts, hashes, NULL, NULL};
   par_for(nq, 16, bh_body, &c);
 }
 
@@ -731,6 +732,8 @@ typedef struct {
   uint64_t seed;
   double *val, *grad;
   int32_t* counts;
+  int rng_mode;               /* sampler only: ORC_RNG_PHILOX or ORC_RNG_MT19937 */
+  const uint32_t* mt_seeds;   /* sampler, mt19937: per-query seeds (NULL: the index) */
 } grad_ctx;
 
 static void bh_grad_body(void* vc, int64_t i) {
@@ -744,7 +747,7 @@ static void bh_grad_body(void* vc, int64_t i) {
 
 void orc_bh_grad(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta,
                  float eps, float alpha, double* val, double* grad, int32_t* counts) {
-  grad_ctx c = {t, kernel, 0, q, beta, eps, alpha, 0, val, grad, counts};
+  grad_ctx c = {t, kernel, 0, q, beta, eps, alpha, 0, val, grad, counts, ORC_RNG_PHILOX, NULL};
   par_for(nq, 16, bh_grad_body, &c);
 }
 
@@ -811,7 +814,8 @@ static void bh_vote_body(void* vc, int64_t g) {
 
 void orc_bh_vote(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta,
                  float eps, int group, float* out, int32_t* counts) {
-  eval_ctx c = {t, kernel, group, 0, 0, q, nq, beta, eps, 0, NULL, out, counts, NULL, NULL};
+  eval_ctx c = {t, kernel, group, 0, 0, q, nq, beta, eps, 0, NULL, out, counts, NULL, NULL,
+                NULL};
   par_for((nq + group - 1) / group, 4, bh_vote_body, &c);
 }
 
@@ -927,9 +931,11 @@ static float rng_uniform(orc_rng* r) {
 
 /* multiLevelPrefixControlVariateSample_stackless, include/tree_sampler.h:21-113. */
 static float sbh_one(const orc_tree* t, int kernel, const float* q, int samples, orc_rng* rng,
-                     float eps, int32_t* total_contribs, double* scale_out) {
+                     float eps, int32_t* total_contribs, double* scale_out,
+                     int32_t* deepest_out) {
   float bh = 0, mlcv = 0;
   int tc = 0;
+  int32_t deepest = 0;
   double scale = 0; /* magnitude of everything summed: sum of |term| x |weight| */
   if (t->leaf[0]) { /* a single-leaf tree has no root children to sample */
     *total_contribs = 0;
@@ -982,6 +988,7 @@ static float sbh_one(const orc_tree* t, int kernel, const float* q, int samples,
           *total_contribs = -1;
           return NAN;
         }
+        if (t->depth[cur] > deepest) deepest = t->depth[cur];
         cb = (cb < ffr) ? ffr : cb; /* std::max(cur_beta, far_field_ratio) */
         float prev_res = kern_node(t, kernel, prev, q, eps);
         float cur_res = 0;
@@ -1016,6 +1023,7 @@ static float sbh_one(const orc_tree* t, int kernel, const float* q, int samples,
   }
   *total_contribs = tc;
   if (scale_out) *scale_out = scale;
+  if (deepest_out) *deepest_out = deepest;
   return bh + mlcv;
 }
 
@@ -1033,7 +1041,7 @@ static void sbh_body(void* vc, int64_t i) {
   }
   int32_t n = 0;
   c->out[i] = sbh_one(c->t, c->kernel, c->q + i * c->t->dim, c->samples, &r, c->eps, &n,
-                      c->scales ? c->scales + i : NULL);
+                      c->scales ? c->scales + i : NULL, c->deepest ? c->deepest + i : NULL);
   if (c->counts) c->counts[i] = n;
 }
 
@@ -1041,8 +1049,18 @@ void orc_sbh(const orc_tree* t, int kernel, const float* q, int64_t nq, int samp
              int rng_mode, uint64_t seed, const uint32_t* mt_seeds, float eps, float* out,
              int32_t* counts, double* scales) {
   eval_ctx c = {t, kernel, 0, samples, rng_mode, q, nq, 0, eps, seed, mt_seeds, out, counts, NULL,
-                scales};
+                scales, NULL};
   par_for(nq, 16, sbh_body, &c);
+}
+
+void orc_sbh_deepest(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
+                     int rng_mode, uint64_t seed, const uint32_t* mt_seeds, float eps,
+                     int32_t* deepest) {
+  float* out = (float*)malloc((size_t)(nq > 0 ? nq : 1) * sizeof(float));
+  eval_ctx c = {t, kernel, 0, samples, rng_mode, q, nq, 0, eps, seed, mt_seeds, out, NULL, NULL,
+                NULL, deepest};
+  par_for(nq, 16, sbh_body, &c);
+  free(out);
 }
 
 /* The stochastic estimator's value and gradient on the Philox paths of
@@ -1140,10 +1158,14 @@ static void sbh_grad_body(void* vc, int64_t i) {
   const int dim = c->t->dim;
   orc_rng r;
   memset(&r, 0, sizeof(r));
-  r.mode = ORC_RNG_PHILOX;
-  r.key[0] = (uint32_t)c->seed;
-  r.key[1] = (uint32_t)(c->seed >> 32);
-  r.query = (uint64_t)i;
+  r.mode = c->rng_mode;
+  if (c->rng_mode == ORC_RNG_MT19937) {
+    mt_seed(&r.mt, c->mt_seeds ? c->mt_seeds[i] : (uint32_t)i);
+  } else {
+    r.key[0] = (uint32_t)c->seed;
+    r.key[1] = (uint32_t)(c->seed >> 32);
+    r.query = (uint64_t)i;
+  }
   int32_t n = 0;
   sbh_grad_one(c->t, c->kernel, c->q + i * dim, c->samples, &r, c->eps, c->alpha, c->val + i,
                c->grad + i * dim, &n);
@@ -1153,7 +1175,16 @@ static void sbh_grad_body(void* vc, int64_t i) {
 void orc_sbh_grad(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
                   uint64_t seed, float eps, float alpha, double* val, double* grad,
                   int32_t* counts) {
-  grad_ctx c = {t, kernel, samples, q, 0, eps, alpha, seed, val, grad, counts};
+  grad_ctx c = {t, kernel, samples, q, 0, eps, alpha, seed, val, grad, counts, ORC_RNG_PHILOX,
+                NULL};
+  par_for(nq, 16, sbh_grad_body, &c);
+}
+
+void orc_sbh_grad_rng(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
+                      int rng_mode, uint64_t seed, const uint32_t* mt_seeds, float eps,
+                      float alpha, double* val, double* grad, int32_t* counts) {
+  grad_ctx c = {t, kernel, samples, q, 0, eps, alpha, seed, val, grad, counts, rng_mode,
+                mt_seeds};
   par_for(nq, 16, sbh_grad_body, &c);
 }
 

@@ -91,6 +91,17 @@ void orc_bh_grad(const orc_tree* t, int kernel, const float* q, int64_t nq, floa
 void orc_sbh_grad(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
                   uint64_t seed, float eps, float alpha, double* val, double* grad,
                   int32_t* counts);
+/* The sampler of orc_sbh, reporting per query only the depth of the deepest
+ * node any of its paths reached (coverage of deep trees in tests). */
+void orc_sbh_deepest(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
+                     int rng_mode, uint64_t seed, const uint32_t* mt_seeds, float eps,
+                     int32_t* deepest);
+/* orc_sbh_grad with the random stream of choice: ORC_RNG_PHILOX (seed, as
+ * orc_sbh_grad) or ORC_RNG_MT19937 (the reference CPU sampler's std::mt19937
+ * stream, seeded per query from mt_seeds, as orc_sbh). */
+void orc_sbh_grad_rng(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
+                      int rng_mode, uint64_t seed, const uint32_t* mt_seeds, float eps,
+                      float alpha, double* val, double* grad, int32_t* counts);
 void orc_brute_force_grad_f64(const float* pts, const float* mass, int64_t n, int dim,
                               int kernel, float alpha, float eps, const float* q, int64_t nq,
                               double* val, double* grad);

@@ -1,0 +1,262 @@
+"""GPU parity at the benchmark's own scale, and the sampler's variance per query.
+
+The small golden trees (at most 65k points) do not reach the depths and path
+codes of the benchmark trees, so these tests run the CUDA path on:
+
+  * the stochastic winding-number workload's tree itself: 1,048,576 points
+    area-uniform on the torus (R 0.6, r 0.2, seed 2024), Octree2 (branching
+    64) for the sampler and Octree1 (branching 8) for Barnes-Hut, with a
+    seeded 2,048-query subset of its 4,194,304 uniform queries;
+  * a torus with clusters of near-duplicate points whose leaves lie deeper than
+    the per-point path codes reach (10 levels in Octree2, 21 in Octree1), with
+    queries at the clusters, so that sampled paths take the geometric
+    containedInChild fallback (include/tree3d.h:172-183).
+
+Sampler parity is against the oracle's restatement of
+multiLevelPrefixControlVariateSample_stackless (include/tree_sampler.h:21-113)
+driven by the same Philox stream: identical contribution counts, values within
+2e-5 of each query's summed magnitude (the GPU adds each node's children as a
+balanced tree, the reference left to right).  Barnes-Hut parity is against the
+oracle's evaluateBarnesHut_stackless (include/barnes_hut.h:23-78): identical
+contribution counts, bit-identical values.
+
+Variance: the north star asks for per-query variance within 10% of the
+reference's at an equal budget.  The reference is the oracle's mt19937 sampler
+(the reference CPU's own std::mt19937 / uniform_real_distribution stream,
+pinned bit for bit by the golden vectors); the GPU draws Philox.  With 16,384
+replicates the noise of a variance ratio is about 2% per query (its standard
+error is estimated from the sample kurtosis of both replicate sets); every
+query whose ratio has a standard error of at most 3.3% must be within 10%
+outright, the others within 10% plus three standard errors, and at least 80%
+of the queries must be in the first group (60% for the heavy-tailed gradient
+of the smooth sum, with four times the replicates).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import sbh_capi as C
+import sbh_workloads as W
+from helpers import bits_equal, sampler_close
+
+pytestmark = pytest.mark.gpu
+
+CONFIG_POINTS = 1 << 20
+CONFIG_QUERIES = 1 << 22
+SUBSET = 2048
+
+
+@pytest.fixture(scope="module")
+def torus_config():
+    pts, nrm, a = W.torus_surface(CONFIG_POINTS, seed=2024)
+    lo, hi = W.padded_box(pts)
+    q_all = W.uniform_queries(CONFIG_QUERIES, seed=4048)
+    q = np.ascontiguousarray(q_all[:: CONFIG_QUERIES // SUBSET][:SUBSET])
+    return pts, nrm, a, lo, hi, q
+
+
+@pytest.fixture(scope="module")
+def octree2(torus_config):
+    pts, nrm, a, lo, hi, _ = torus_config
+    gpu = C.GpuTree(C.HostTree(pts, nrm, a, lo, hi, dim_split_log=2))
+    ot = O.OracleTree(pts, nrm, a, lo, hi, dim_split_log=2)
+    return gpu, ot
+
+
+@pytest.fixture(scope="module")
+def octree1(torus_config):
+    pts, nrm, a, lo, hi, _ = torus_config
+    gpu = C.GpuTree(C.HostTree(pts, nrm, a, lo, hi, dim_split_log=1))
+    ot = O.OracleTree(pts, nrm, a, lo, hi, dim_split_log=1)
+    return gpu, ot
+
+
+# ------------------------------------------------------ the config-2 tree
+
+@pytest.mark.parametrize("kernel,samples,seed", [(C.WINDING_NUMBER, 4, 1234),
+                                                 (C.GRAVITY, 1, 7),
+                                                 (C.WINDING_NUMBER, 16, 99)])
+def test_sampler_on_config_tree_matches_oracle(torus_config, octree2, kernel, samples, seed):
+    q = torus_config[-1]
+    gpu, ot = octree2
+    assert gpu.info.num_points == CONFIG_POINTS and gpu.info.root_children == 64
+    rv, rc, sc = ot.sbh(kernel, q, samples, rng=O.RNG_PHILOX, seed=seed, return_scale=True)
+    v, _, cnt = gpu.eval(q, C.params(method=C.STOCHASTIC, kernel=kernel,
+                                     samples_per_subdomain=samples, seed=seed), contribs=True)
+    assert np.array_equal(cnt, rc)
+    assert sampler_close(v, rv, sc), np.abs(v - rv).max()
+
+
+@pytest.mark.parametrize("tree", ["octree1", "octree2"])
+@pytest.mark.parametrize("kernel", [C.WINDING_NUMBER, C.GRAVITY])
+@pytest.mark.parametrize("theta", [0.5, 0.3])
+def test_barnes_hut_on_config_tree_bitwise(request, torus_config, tree, kernel, theta):
+    q = torus_config[-1]
+    gpu, ot = request.getfixturevalue(tree)
+    beta = 1.0 / theta
+    rv, rc, _ = ot.bh(kernel, q, beta)
+    v, _, cnt = gpu.eval(q, C.params(method=C.BARNES_HUT, kernel=kernel, beta=beta),
+                         contribs=True)
+    assert np.array_equal(cnt, rc)
+    assert bits_equal(v, rv), np.abs(v - rv).max()
+
+
+# ------------------------------------- paths beyond the per-point path codes
+
+def _deep_cluster_tree():
+    """16,384 torus points plus 8 clusters of 64 points with spreads 1e-5..3e-7:
+    the clusters' leaves lie 13 levels down in Octree2 and 24 in Octree1, past
+    the 10 / 21 levels a 63-bit path code holds."""
+    pts, nrm, a = W.torus_surface(16384, seed=91)
+    rng = np.random.default_rng(92)
+    centres = pts[rng.integers(0, len(pts), 8)]
+    spreads = (1e-5, 5e-6, 3e-6, 2e-6, 1e-6, 7e-7, 5e-7, 3e-7)
+    cl = [c + rng.normal(0, s, (64, 3)) for c, s in zip(centres, spreads)]
+    P = np.concatenate([pts] + cl).astype(np.float32)
+    N = np.concatenate([nrm, np.tile(nrm[:1], (512, 1))]).astype(np.float32)
+    A = np.concatenate([a, np.full(512, a[0])]).astype(np.float32)
+    q = (np.concatenate(cl)[rng.integers(0, 512, 512)] +
+         rng.normal(0, 1e-6, (512, 3))).astype(np.float32)
+    return P, N, A, q
+
+
+@pytest.mark.parametrize("dsl,samples", [(2, 16), (1, 64)])
+@pytest.mark.parametrize("kernel", [C.WINDING_NUMBER, C.GRAVITY])
+def test_sampler_paths_past_the_path_codes(dsl, samples, kernel):
+    P, N, A, q = _deep_cluster_tree()
+    lo, hi = W.padded_box(P)
+    gpu = C.GpuTree(C.HostTree(P, N, A, lo, hi, dim_split_log=dsl))
+    ot = O.OracleTree(P, N, A, lo, hi, dim_split_log=dsl)
+    code_levels = 63 // (3 * dsl)
+    assert gpu.info.depth > code_levels
+    # Coverage: many queries have a path that goes deeper than the codes reach.
+    deep = ot.sbh_deepest(kernel, q, samples, seed=5)
+    assert (deep > code_levels).sum() >= 64
+    rv, rc, sc = ot.sbh(kernel, q, samples, rng=O.RNG_PHILOX, seed=5, return_scale=True)
+    v, _, cnt = gpu.eval(q, C.params(method=C.STOCHASTIC, kernel=kernel,
+                                     samples_per_subdomain=samples, seed=5), contribs=True)
+    assert np.array_equal(cnt, rc)
+    assert sampler_close(v, rv, sc)
+    # Barnes-Hut on the same deep tree, bit for bit.
+    bv, bc, _ = ot.bh(kernel, q, 2.0)
+    g, _, gc = gpu.eval(q, C.params(method=C.BARNES_HUT, kernel=kernel, beta=2.0), contribs=True)
+    assert np.array_equal(gc, bc)
+    assert bits_equal(g, bv)
+
+
+# ------------------------------------------------- per-query variance
+
+REPS = 16384
+STRICT_SE = 0.033
+
+
+def variance_with_noise(x):
+    """Per-column sample variance and the relative standard error of that
+    variance, sqrt(2/(n-1) + (kurtosis-3)/n), from the sample's own kurtosis."""
+    n = x.shape[0]
+    d = x - x.mean(0)
+    s2 = (d ** 2).sum(0) / (n - 1)
+    kurt = (d ** 4).mean(0) / np.maximum(s2 ** 2, 1e-300)
+    return s2, np.sqrt(np.maximum(2.0 / (n - 1) + (kurt - 3.0) / n, 0.0))
+
+
+def check_variance_ratios(gpu_reps, ref_reps, min_strict=0.8):
+    vg, rg = variance_with_noise(gpu_reps)
+    vr, rr = variance_with_noise(ref_reps)
+    live = vr > 0
+    assert np.array_equal(vg > 0, live)
+    ratio = vg[live] / vr[live]
+    se = np.sqrt(rg[live] ** 2 + rr[live] ** 2)
+    strict = se <= STRICT_SE
+    assert strict.mean() >= min_strict, strict.mean()
+    assert np.all(np.abs(ratio[strict] - 1.0) <= 0.10), ratio[strict]
+    assert np.all(np.abs(ratio - 1.0) <= 0.10 + 3.0 * se), (ratio, se)
+    return ratio
+
+
+def _variance_workload(name):
+    if name == "torus_wn":
+        pts, nrm, m = W.torus_surface(4000, seed=51)
+        return pts, nrm, m, C.WINDING_NUMBER, 3
+    if name == "gauss_gravity":
+        pts, nrm, m = W.gaussian_mixture(4000, seed=52)
+        return pts, nrm, m, C.GRAVITY, 3
+    pts, nrm, m = W.circle_points(4000, seed=53)
+    return pts, nrm, m, C.WINDING_NUMBER, 2
+
+
+def _mt_seeds(n):
+    return (np.arange(n, dtype=np.uint64) * 2654435761 % (2 ** 32)).astype(np.uint32)
+
+
+@pytest.mark.parametrize("workload", ["torus_wn", "gauss_gravity", "circle_wn2d"])
+@pytest.mark.parametrize("samples", [1, 4])
+def test_sampler_variance_per_query_matches_reference(workload, samples):
+    pts, nrm, m, kernel, dim = _variance_workload(workload)
+    lo, hi = W.padded_box(pts)
+    gpu = C.GpuTree(C.HostTree(pts, nrm, m, lo, hi, dim_split_log=2))
+    q = W.uniform_queries(32, seed=54, dim=dim)
+    qq = np.tile(q, (REPS, 1))  # every replicate has its own query index: independent streams
+    v, _ = gpu.eval(qq, C.params(method=C.STOCHASTIC, kernel=kernel,
+                                 samples_per_subdomain=samples, seed=99))
+    ot = O.OracleTree(pts, nrm, m, lo, hi, dim_split_log=2)
+    rv, _ = ot.sbh(kernel, qq, samples, rng=O.RNG_MT19937, mt_seeds=_mt_seeds(len(qq)))
+    check_variance_ratios(v.reshape(REPS, -1).astype(np.float64),
+                          rv.reshape(REPS, -1).astype(np.float64))
+
+
+@pytest.mark.parametrize("kernel", [C.GRAVITY, C.SMOOTH_DIST])
+def test_sampler_gradient_variance_per_query_matches_reference(kernel):
+    """Budget 128 (2 paths in each of the 64 root children): the GPU adjoint's
+    gradient estimates against the reference estimator's (the oracle's gradient
+    over the reference's mt19937 paths), per query and component.  Gravity: the
+    potential's gradient; smooth distance: the gradient of the sum
+    S = exp(-alpha D), recovered from (D, dD/dq) as -alpha S dD/dq."""
+    pts, nrm, m = W.torus_surface(4000, seed=56, jitter=1e-3)
+    alpha = 20.0
+    lo, hi = W.padded_box(pts)
+    gpu = C.GpuTree(C.HostTree(pts, nrm, m, lo, hi, alpha=alpha, dim_split_log=2))
+    assert gpu.info.root_children == 64
+    samples = 2
+    # The smooth sum's gradient is heavy-tailed (rare paths close to the query
+    # carry large weights): four times the replicates, and at least 60% of the
+    # queries in the strict group.
+    reps, min_strict = (REPS, 0.8) if kernel == C.GRAVITY else (4 * REPS, 0.6)
+    q = W.uniform_queries(16, seed=57, dim=3, lo=-0.9, hi=0.9)
+    qq = np.tile(q, (reps, 1))
+    v, g, _ = gpu.eval_grad(qq, C.params(method=C.STOCHASTIC, kernel=kernel,
+                                         samples_per_subdomain=samples, seed=3, alpha=alpha))
+    ot = O.OracleTree(pts, nrm, m, lo, hi, alpha=alpha, dim_split_log=2)
+    rv, rg, _ = ot.sbh_grad(kernel, qq, samples, alpha=alpha, rng=O.RNG_MT19937,
+                            mt_seeds=_mt_seeds(len(qq)))
+    g = g.astype(np.float64)
+    if kernel == C.SMOOTH_DIST:
+        ok = np.isfinite(v) & np.isfinite(rv)
+        assert ok.mean() > 0.999
+        s_gpu = np.exp(-alpha * v.astype(np.float64))[:, None]
+        s_ref = np.exp(-alpha * rv)[:, None]
+        g = -alpha * s_gpu * g
+        rg = -alpha * s_ref * rg
+        g[~ok] = 0.0
+        rg[~ok] = 0.0
+    for k in range(3):
+        check_variance_ratios(g[:, k].reshape(reps, -1), rg[:, k].reshape(reps, -1), min_strict)
+
+
+# ------------------------------------------- the FP64 accuracy reference
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kernel", [C.GRAVITY, C.WINDING_NUMBER, C.SMOOTH_DIST, C.PLUMMER])
+def test_gpu_fp64_brute_force_matches_cpu_fp64(dim, kernel):
+    """The oracle's GPU FP64 brute force (the accuracy reference of the
+    benchmark) equals the CPU FP64 oracle to FP64 rounding."""
+    if dim == 3:
+        pts, nrm, m = W.torus_surface(20000, seed=61, jitter=1e-3)
+    else:
+        pts, nrm, m = W.circle_points(20000, seed=62)
+    q = W.uniform_queries(1500, seed=63, dim=dim, lo=-1.2, hi=1.2)
+    for abs_sum in (False, True):
+        a = O.gpu_brute_force_f64(pts, nrm, m, kernel, q, alpha=30.0, abs_sum=abs_sum)
+        b = O.brute_force_f64(pts, nrm, m, kernel, q, alpha=30.0, abs_sum=abs_sum)
+        scale = O.brute_force_f64(pts, nrm, m, kernel, q, alpha=30.0, abs_sum=True)
+        assert np.all(np.abs(a - b) <= 1e-12 * scale), np.abs(a - b).max()

@@ -141,3 +141,10 @@ def test_brute_force_f64_analytic():
         -2.0 / (1.0 + float(np.float32(0.1))), rel=1e-7)
     assert O.brute_force_f64(p, n, m, O.SMOOTH_DIST, q, alpha=3.0)[0] == pytest.approx(np.exp(-3.0),
                                                                                    rel=1e-7)
+
+
+def test_gpu_fp64_brute_force_library_loads():
+    """The FP64 GPU brute force (the benchmark's accuracy reference) is built
+    and exports its entry point; running it needs a GPU."""
+    lib = O.gpu_lib()
+    assert hasattr(lib, "orc_gpu_brute_force_f64")

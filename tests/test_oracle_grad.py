@@ -122,6 +122,29 @@ def test_sampler_gradient_walks_the_plain_sampler_paths(dim, kernel):
     assert np.all(np.isfinite(grad[np.isfinite(val)]))
 
 
+@pytest.mark.parametrize("kernel", GRAD_KERNELS)
+def test_sampler_gradient_on_the_reference_mt19937_stream(kernel):
+    """With the reference CPU sampler's std::mt19937 stream (seeded per query),
+    the gradient oracle walks the same paths as orc_sbh on that stream: same
+    contribution counts, and values agree to the FP32-vs-FP64 rounding."""
+    pts, nrm, m = _points(3, 4000, seed=74)
+    lo, hi = W.padded_box(pts)
+    t = O.OracleTree(pts, nrm, m, lo, hi, alpha=25.0, dim_split_log=2)
+    q = np.random.default_rng(75).uniform(-1.0, 1.0, (200, 3)).astype(np.float32)
+    seeds = np.arange(200, dtype=np.uint32) * 7919 + 3
+    val, grad, cnt = t.sbh_grad(kernel, q, 2, alpha=25.0, rng=O.RNG_MT19937, mt_seeds=seeds)
+    pv, pc = t.sbh(kernel, q, 2, rng=O.RNG_MT19937, mt_seeds=seeds)
+    assert np.array_equal(cnt, pc)
+    if kernel == O.SMOOTH_DIST:
+        ok = pv > 0
+        assert np.allclose(val[ok], -np.log(pv[ok].astype(np.float64)) / 25.0, rtol=1e-4)
+    else:
+        assert np.allclose(val, pv, rtol=1e-4)
+    # a different stream takes different paths
+    _, _, cnt2 = t.sbh_grad(kernel, q, 2, alpha=25.0, rng=O.RNG_MT19937, mt_seeds=seeds + 1)
+    assert not np.array_equal(cnt, cnt2)
+
+
 def test_sampler_gravity_gradient_is_unbiased():
     """Mean of the stochastic gravity gradient over 512 seeds equals the exact
     gradient within 4 standard errors, per query and component."""
