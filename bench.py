@@ -1,29 +1,41 @@
 """Benchmark of the stochastic Barnes-Hut summation path on B200.
 
-Default workload (the configuration the headline metric is quoted on):
-stochastic Barnes-Hut winding number in 3D -- 1,048,576 oriented points sampled
-area-uniformly on a torus (R=0.6, r=0.2) with exact normals and area weights
-4 pi^2 R r / N, an Octree2-type tree (branching 64, leaf size 1, the reference's
-recommended tree for the sampler), 4,194,304 queries uniform in [-1,1]^3, and a
-budget of 256 sampled paths per query (samples_per_subdomain = 256 / root
-children).  A step is one evaluation of all queries.
+Default workload (the configuration the headline metric is quoted on): serving.
+32 resident trees (16 3D, 16 2D; Gaussian mixtures, torus, sphere and circle
+surfaces; 10^4..2*10^6 points) and 1,500 seeded requests (a tree, a kernel --
+gravity, winding number or smooth distance with alpha 100 --, 1..10^5 queries in
+the tree's box, a sample budget 64/256/1024).  Both paths run at matched
+accuracy, median relative error <= 1e-3 against FP64 brute force per kernel:
+the plain per-call Barnes-Hut drop-in at each kernel's matched theta, the
+served path at each kernel's matched operating point (stochastic BH with the
+drawn budgets scaled per kernel, or Barnes-Hut where the stochastic estimate
+cannot reach the target); the errors are re-measured in every run.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sbh_wn|bh_wn|plain_small_bf|plain_small_bh|differentiation|
-                                batching|serving|tree_build] [--nq N] [--budget B]
+                    [--workload serving|sbh_wn|bh_wn|plain_small_bf|plain_small_bh|
+                                differentiation|batching|tree_build] [--calibrate]
 
-`value` is queries/s with queries already resident in HBM (device-pointer C ABI
-call: Morton bucketing + sampler kernel), timed with CUDA events per step, L2
-flushed between steps.  `e2e` is the same through the blocking C ABI call with
-pinned host buffers (host->device copy, evaluation, device->host copy inside
-the timed region).  Under torchrun every rank evaluates its own query batch
-against its own replica of the tree (replicas only: the path has no exchange
-step); `value` is all ranks' queries over the slowest rank's time.
+Serving line: `value` is queries/s of the whole request stream evaluated as one
+batch with every request's queries resident in HBM (CUDA events, L2 flushed
+between steps); `e2e` the same stream through the server's C ABI (host buffers
+in and out, continuous batching, every request submitted at t = 0), with p50 /
+p99 latency; `plain_barnes_hut` the reference-style one blocking call per
+request; `served_over_plain` their ratio; `latency_at_rates` p50 / p99 under
+Poisson arrivals at 0.5x, 1x and 2x the plain path's capacity.
 
-`--impl reference` times the reference's own CPU implementation
-(src/sbh.cpp multiLevelPrefixControlVariateSampler, compiled unmodified in
-oracle/_ref) on the same workload, on bounded query samples, with all host
-threads; under torchrun only rank 0 runs it.
+Single-configuration workloads (sbh_wn, bh_wn, plain_small_*): `value` is
+queries/s with queries resident in HBM (Morton bucketing + kernel), `e2e` the
+blocking C ABI call with pinned host buffers, `e2e_plugin` the reference's own
+Python call (`sbh_gpu`) with a float64 NumPy array.  Under torchrun every rank
+evaluates its own query batch against its own replica of the tree (replicas
+only: the path has no exchange step); `value` is all ranks' queries over the
+slowest rank's time.
+
+`--impl reference` times the reference's own CPU implementation (src/sbh.cpp,
+compiled unmodified in oracle/_ref) on the same workload and operating points,
+on bounded samples, with all host threads; under torchrun only rank 0 runs it.
+Accuracy figures come from the oracle's FP64 GPU brute force, outside every
+timed region.
 """
 from __future__ import annotations
 
@@ -48,15 +60,27 @@ FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 512 << 20
 
 # DRAM bytes (read + written) of one launch of each workload's main kernel at
-# its default size, from a single-pass ncu capture of the same bench command
-# (dram__bytes_read.sum + dram__bytes_write.sum, --clock-control none; the
-# commands and figures are in profiles/dram_traffic_full_launches.md).  Null in
-# the bench line when the query count or budget is overridden.
+# its default size: dram__bytes_read.sum + dram__bytes_write.sum from a
+# single-pass ncu capture of the same bench command (--clock-control none).
+# Recaptured after every change to the kernel; the capture command and the
+# figures are listed with the kernel's profile.  Null in the bench line when
+# the query count or budget is overridden.
 DRAM_TRAFFIC = {
-    "sbh_wn": 4.39e9 + 208.95e6,
+    "sbh_wn": None,
     "bh_wn": 307.58e6 + 31.53e6,
     "plain_small_bf": 1.85e6,
     "plain_small_bh": 3.36e6,
+}
+
+# What each single-configuration workload measures (the headline metric is the
+# serving workload's).
+WORKLOAD_METRIC = {
+    "sbh_wn": "stochastic BH winding-number queries/s (1,048,576-point torus, 4,194,304 "
+              "queries, 256 paths/query)",
+    "bh_wn": "deterministic BH winding-number queries/s (1,048,576-point torus, 4,194,304 "
+             "queries, theta 0.5)",
+    "plain_small_bf": "brute-force Plummer queries/s (65,536 x 65,536)",
+    "plain_small_bh": "deterministic BH Plummer queries/s (65,536 x 65,536, theta 0.5, leaf 8)",
 }
 
 WORKLOADS = {
@@ -237,6 +261,36 @@ def dram_traffic(wl):
     return DRAM_TRAFFIC.get(wl.get("name"))
 
 
+def timed_device(fn, stream, flush, warmup, steps):
+    """Event-timed runs of fn() on `stream`, L2 flushed before each; ms per run."""
+    import torch
+    for _ in range(warmup):
+        flush.zero_()
+        fn()
+    ev = []
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def sampler_load_bytes(info_l2, leaf_points, nq, paths, deeper_terms):
+    """Global-memory bytes the stochastic kernel's loads request per launch,
+    from its own counts: the first-level records (32 B each: centroid/diameter
+    and aggregate) staged once per warp of 32 queries; per sampled path its
+    subdomain's topology (16 B), the sample's path code (8 B), the subdomain's
+    centroid (16 B), its child mask (8 B) and the topology and centroid of the
+    node the first step reaches (32 B); 32 B per deeper kernel term."""
+    units = (nq + 31) // 32
+    return units * (info_l2 + leaf_points) * 32 + nq * paths * 80 + deeper_terms * 32
+
+
 def run_ours(args, wl):
     import torch
 
@@ -265,7 +319,8 @@ def run_ours(args, wl):
     nq = q.shape[0]
     samples = W.samples_for_budget(wl.get("budget", 1), info.root_children)
     p = C.params(method=method_id(C, wl["method"]), kernel=kernel_id(C, wl["kernel"]),
-                 beta=wl.get("beta", 2.0), samples_per_subdomain=samples, seed=1234)
+                 beta=wl.get("beta", 2.0), samples_per_subdomain=samples, seed=1234,
+                 flags=C.FLAG_STAGE_LEAVES if args.stage_leaves else 0)
 
     d_q = torch.from_numpy(np.ascontiguousarray(q.T)).to(dev)  # SoA [3][nq]
     d_out = torch.empty(nq, dtype=torch.float32, device=dev)
@@ -275,7 +330,7 @@ def run_ours(args, wl):
     def step_device():
         gpu.eval_device(d_q.data_ptr(), nq, d_out.data_ptr(), p, stream=s_handle)
 
-    # Work counts (untimed): contributions per query define the algorithmic bytes.
+    # Work counts (untimed): contributions per query (the reference's count).
     gpu.eval_device(d_q.data_ptr(), nq, d_out.data_ptr(), p, stream=s_handle,
                     d_contribs=d_cnt.data_ptr())
     gpu.check(s_handle)
@@ -307,25 +362,14 @@ def run_ours(args, wl):
     step_ms = [a.elapsed_time(b) for a, b in times]
     total_ms = float(sum(step_ms))
 
-    # Dominant kernel alone: the sampler on pre-bucketed queries (no sort launch).
+    # Dominant kernel alone: the evaluation on pre-bucketed queries (no sort launch).
     order = morton_order(q)
     d_qs = torch.from_numpy(np.ascontiguousarray(q[order].T)).to(dev)
     pk = C.params(method=p.method, kernel=p.kernel, beta=p.beta, samples_per_subdomain=samples,
-                  seed=p.seed, flags=C.FLAG_KEEP_ORDER)
-    for _ in range(max(1, args.warmup)):
-        flush.zero_()
-        gpu.eval_device(d_qs.data_ptr(), nq, d_out.data_ptr(), pk, stream=s_handle)
-    kern_ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        gpu.eval_device(d_qs.data_ptr(), nq, d_out.data_ptr(), pk, stream=s_handle)
-        e1.record(stream)
-        kern_ms.append((e0, e1))
-    torch.cuda.synchronize(dev)
-    kern_ms = [a.elapsed_time(b) for a, b in kern_ms]
+                  seed=p.seed, flags=p.flags | C.FLAG_KEEP_ORDER)
+    kern_ms = timed_device(lambda: gpu.eval_device(d_qs.data_ptr(), nq, d_out.data_ptr(), pk,
+                                                   stream=s_handle),
+                           stream, flush, max(1, args.warmup), args.steps)
 
     # End to end through the blocking C ABI call with pinned host buffers.
     h_q = torch.from_numpy(np.ascontiguousarray(q.T)).pin_memory()
@@ -347,8 +391,13 @@ def run_ours(args, wl):
     torch.cuda.synchronize(dev)
     e2e_ms = float(sum(a.elapsed_time(b) for a, b in e2e))
 
-    # Accuracy on a query subset against brute force, and the deterministic
-    # Barnes-Hut comparison the workload prescribes (Octree1, theta 0.3/0.5/0.8).
+    # End to end through the reference's own Python call: the `sbh_gpu` module
+    # with a NumPy float64 (n, 3) array, as the reference's callers pass it
+    # (pageable memory, float64 -> float32 conversion and layout change inside).
+    plugin = plugin_e2e(wl, pts, nrm, m, lo, hi, q, samples, args)
+
+    # Accuracy on a query subset against FP64 brute force, and (stochastic) the
+    # Pareto comparison with deterministic Barnes-Hut the workload prescribes.
     accuracy = compare = None
     if not args.no_accuracy:
         accuracy, compare = accuracy_report(C, torch, wl, gpu, p, pts, nrm, m, lo, hi, d_q, nq,
@@ -360,11 +409,9 @@ def run_ours(args, wl):
     if rank != 0:
         return None
 
-    bytes_per_eval = 32 if wl["kernel"] == "wn" else 16
-    alg_bytes = contribs * bytes_per_eval + nq * 16
     kmean_s = statistics.mean(kern_ms) / 1e3
     peak, peak_kind = load_peaks()
-    achieved = alg_bytes / kmean_s / 1e9
+    traffic = dram_traffic(wl)
     if wl["method"] == "brute_force":
         # Brute force is bound by the MUFU pipe: one rsqrt per Plummer pair (two
         # MUFU ops -- rsqrt and reciprocal -- for gravity and the winding number).
@@ -379,14 +426,44 @@ def run_ours(args, wl):
                            f"{rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
                            f"{rates['sm_clock_mhz']:.0f} MHz; {mufu_per_pair} MUFU op(s) per pair",
             "kernel_ms": statistics.mean(kern_ms), "pairs_per_launch": pairs,
-            "pipe_rates": rates, "traffic": dram_traffic(wl),
+            "pipe_rates": rates, "traffic": traffic,
         }
     else:
-        roofline = None
+        if wl["method"] == "stochastic":
+            l2, terms, internal, leafpts = sampler_first_level(host)
+            first = nq * (samples * terms + internal + leafpts)
+            deeper = max(0, contribs - first)
+            alg = sampler_load_bytes(l2, leafpts, nq, samples * info.root_children, deeper)
+            definition = ("global-memory bytes the kernel's loads request, from its own counts: "
+                          "first-level records 32 B each once per 32 queries, 80 B per sampled "
+                          "path's first step, 32 B per deeper kernel term")
+            kernel_name = "stochastic_kernel"
+        else:
+            bpe = 32 if wl["kernel"] == "wn" else 16
+            alg = contribs * bpe + nq * 16
+            definition = (f"{bpe} B per kernel evaluation (node or point record) + 16 B per "
+                          "query (SURVEY 8(d) per-unit figure; the opening tests' 32 B reads are "
+                          "not counted)")
+            kernel_name = "barnes_hut_kernel"
+        roofline = {
+            "bound": "issue", "kernel": kernel_name,
+            "achieved": alg / kmean_s / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": alg / kmean_s / 1e9 / peak,
+            "peak_source": (f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
+                            if peak_kind == "measured" else "fallback 6650 GB/s"),
+            "kernel_ms": statistics.mean(kern_ms),
+            "algorithmic_bytes": alg, "bytes_definition": definition,
+            "traffic": traffic,
+            "dram_gbs": None if traffic is None else traffic / kmean_s / 1e9,
+            "dram_frac": None if traffic is None else traffic / kmean_s / 1e9 / peak,
+            "note": "issue- and latency-bound (ncu: the traversal's records come from L1/L2; "
+                    "DRAM traffic is a small fraction of HBM bandwidth); achieved/frac are the "
+                    "requested load bandwidth against the HBM roof, dram_frac the DRAM share",
+        }
     launches_per_step = {"stochastic": 6, "barnes_hut": 6, "brute_force": 1}[wl["method"]]
     clk = clocks.summary()
     out = {
-        "metric": METRIC,
+        "metric": WORKLOAD_METRIC[wl["name"]],
         "value": whole_job_rate(world, nq, total_ms, args.steps),
         "unit": "queries/s",
         "n_gpus": world,
@@ -398,34 +475,21 @@ def run_ours(args, wl):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded generators; the reference publishes no dataset)",
-        "config": {
-            "workload": wl["desc"],
-            "method": wl["method"], "kernel": wl["kernel"], "points": wl["n"],
-            "queries_per_gpu": nq, "tree": f"dim 3, dim_split_log {wl['dsl']}, leaf {wl['leaf']}",
-            "tree_nodes": info.num_nodes, "root_children": info.root_children,
-            "samples_per_subdomain": samples if wl["method"] == "stochastic" else None,
-            "paths_per_query": samples * info.root_children if wl["method"] == "stochastic" else None,
-            "beta": wl.get("beta"),
-            "mean_kernel_evals_per_query": contribs / nq,
-            "host_build_s": round(build_s, 3),
-            "l2": "512 MiB buffer written between timed steps; tree+queries exceed L2 as well",
-            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-        },
+        "config": dict(workload_config(wl, info.num_nodes, info.root_children, samples),
+                       **({"leaf_staging": "bulk asynchronous copies (SBH_FLAG_STAGE_LEAVES)"}
+                          if args.stage_leaves else {})),
+        "work": {"mean_kernel_evals_per_query_reference_count": contribs / nq,
+                 "host_build_s": round(build_s, 3)},
         "e2e": {"value": whole_job_rate(world, nq, e2e_ms, args.steps), "unit": "queries/s",
                 "h2d_bytes_per_step": nq * 12, "d2h_bytes_per_step": nq * 4,
-                "ms_per_step": e2e_ms / args.steps},
-        "roofline": roofline or {
-            "bound": "hbm", "kernel": "stochastic_kernel" if wl["method"] == "stochastic" else wl["method"],
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-            "kernel_ms": statistics.mean(kern_ms),
-            "algorithmic_bytes": alg_bytes,
-            "bytes_definition": f"{bytes_per_eval} B per kernel evaluation (source or node record) + 16 B per query",
-            "traffic": dram_traffic(wl),
-        },
+                "ms_per_step": e2e_ms / args.steps,
+                "path": "sbh_eval (C ABI), pinned float32 SoA host buffers"},
+        "roofline": roofline,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }
+    if plugin is not None:
+        out["e2e_plugin"] = plugin
     if accuracy is not None:
         out["accuracy"] = accuracy
         out["compare"] = compare
@@ -433,6 +497,75 @@ def run_ours(args, wl):
         out["cpu_baseline"] = cpu_baseline(wl, pts, nrm, m, lo, hi, q, samples,
                                            budget_s=args.cpu_seconds)
     return out
+
+
+def workload_config(wl, num_nodes, root_children, samples):
+    """The configuration keys both arms report (identical for the same workload)."""
+    return {
+        "workload": wl["desc"],
+        "method": wl["method"], "kernel": wl["kernel"], "points": wl["n"],
+        "queries_per_gpu": wl["nq"], "tree": f"dim 3, dim_split_log {wl['dsl']}, leaf {wl['leaf']}",
+        "tree_nodes": num_nodes, "root_children": root_children,
+        "samples_per_subdomain": samples if wl["method"] == "stochastic" else None,
+        "paths_per_query": samples * root_children if wl["method"] == "stochastic" else None,
+        "beta": wl.get("beta"),
+        "l2": "512 MiB buffer written between timed steps; tree+queries exceed L2 as well",
+    }
+
+
+def sampler_first_level(host):
+    """The root's first level as the sampler sums it: (records in the range of
+    the root's grandchildren, kernel terms they stand for -- a leaf record
+    holding several points, or none, stands for its points --, internal root
+    children, points of leaf root children)."""
+    n = host.export_nodes()
+    kids = np.nonzero(n["parent"] == 0)[0]
+    kids = kids[kids != 0]
+    leaf = n["is_leaf"][kids].astype(bool)
+    internal = kids[~leaf]
+    grand = np.isin(n["parent"], internal)
+    grand[0] = False
+    pts = n["end"][grand] - n["start"][grand]
+    terms = np.where(n["is_leaf"][grand].astype(bool), pts, 1)
+    leafpts = int((n["end"][kids[leaf]] - n["start"][kids[leaf]]).sum())
+    return int(grand.sum()), int(terms.sum()), int(len(internal)), leafpts
+
+
+def plugin_e2e(wl, pts, nrm, m, lo, hi, q, samples, args):
+    """Wall-clock of the reference-facing Python call (`sbh_gpu`, blocking)
+    with a float64 (n, 3) NumPy array, the form the reference's callers use."""
+    import sbh
+    import sbh_gpu
+    cls = {1: "Octree1", 2: "Octree2", 3: "Octree3"}[wl["dsl"]]
+    if wl["leaf"] != 1:
+        return None
+    h = getattr(sbh, cls)(pts, nrm, m, lo, hi)
+    g = getattr(sbh_gpu, cls.replace("Octree", "OctreeGPU"))(h)
+    q64 = q.astype(np.float64)
+    suffix = {"wn": "wn", "gravity": "gravity", "smooth": "smoothdist"}.get(wl["kernel"])
+    if suffix is None:
+        return None
+    if wl["method"] == "stochastic":
+        fn = lambda: getattr(sbh_gpu, "multi_level_prefix_control_variate_" + suffix)(
+            g, q64, samples)
+        call = f"sbh_gpu.multi_level_prefix_control_variate_{suffix}(tree, q, {samples})"
+    elif wl["method"] == "barnes_hut":
+        fn = lambda: getattr(sbh_gpu, "eval_barnes_hut_" + suffix)(g, q64, wl.get("beta", 2.0))
+        call = f"sbh_gpu.eval_barnes_hut_{suffix}(tree, q, {wl.get('beta', 2.0)})"
+    else:
+        fn = lambda: getattr(sbh_gpu, "eval_brute_force_" + suffix)(g, q64)
+        call = f"sbh_gpu.eval_brute_force_{suffix}(tree, q)"
+    for _ in range(max(1, args.warmup // 2)):
+        fn()
+    steps = max(2, args.steps // 4)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        fn()
+    secs = (time.perf_counter() - t0) / steps
+    return {"value": len(q) / secs, "unit": "queries/s", "ms_per_step": secs * 1e3,
+            "h2d_bytes_per_step": len(q) * 12, "d2h_bytes_per_step": len(q) * 4,
+            "call": call + " with q a C-ordered float64 (n, 3) NumPy array; host wall clock",
+            "steps": steps}
 
 
 ACCURACY_SUBSET = 65536
@@ -448,53 +581,61 @@ def rel_errors(kernel, est, ref):
     return np.abs(est - ref) / np.abs(ref)
 
 
+def fp64_reference(pts, nrm, m, kernel, q, alpha=1.0):
+    """FP64 brute force on the GPU, from the oracle (libsbh_bf64.so): the
+    accuracy reference, computed outside every timed region."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    kid = {"gravity": O.GRAVITY, "wn": O.WINDING_NUMBER, "smooth": O.SMOOTH_DIST,
+           "plummer": O.PLUMMER}[kernel]
+    return O.gpu_brute_force_f64(pts, nrm, m, kid, q, alpha=alpha)
+
+
 def accuracy_report(C, torch, wl, gpu, p, pts, nrm, m, lo, hi, d_q, nq, s_handle, args):
     dev = d_q.device
     n_sub = min(ACCURACY_SUBSET, nq)
+    q_sub = d_q[:, :n_sub].t().contiguous().cpu().numpy()
+    ref = fp64_reference(pts, nrm, m, wl["kernel"], q_sub)
     d_sub = d_q[:, :n_sub].contiguous()
-    ref = torch.empty(n_sub, dtype=torch.float32, device=dev)
-    kid = kernel_id(C, wl["kernel"])
-    gpu.eval_device(d_sub.data_ptr(), n_sub, ref.data_ptr(),
-                    C.params(method=C.BRUTE_FORCE, kernel=kid), stream=s_handle)
     est = torch.empty(n_sub, dtype=torch.float32, device=dev)
     gpu.eval_device(d_sub.data_ptr(), n_sub, est.data_ptr(), p, stream=s_handle)
     torch.cuda.synchronize(dev)
-    ref_np = ref.cpu().numpy().astype(np.float64)
-    e = rel_errors(wl["kernel"], est.cpu().numpy(), ref_np)
+    e = rel_errors(wl["kernel"], est.cpu().numpy(), ref)
     accuracy = {"median_rel_err": float(np.median(e)), "p99_rel_err": float(np.percentile(e, 99)),
                 "subset_queries": n_sub,
-                "reference": "compensated FP32 brute force (within 1e-6 of FP64 by test)",
+                "reference": "FP64 brute force on the GPU (the oracle's libsbh_bf64.so)",
                 "definition": ("|est-ref|/max(|ref|,1)" if wl["kernel"] == "wn"
                                else "|est-ref|/|ref|")}
     compare = {}
     if wl["method"] != "stochastic":
         return accuracy, compare
+    # Pareto comparison on the same queries: the sampler at budgets 64-1024 on
+    # this tree, deterministic Barnes-Hut at theta 0.3/0.5/0.8 on Octree1 (the
+    # reference's recommended tree for it); throughput on all queries
+    # (device-resident, sort included), errors on the subset.
     host1 = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=1, leaf_size=1)
     gpu1 = C.GpuTree(host1, device=dev.index or 0)
     out = torch.empty(nq, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
-    for theta in (0.3, 0.5, 0.8):
-        pb = C.params(method=C.BARNES_HUT, kernel=kid, beta=1.0 / theta)
-        for _ in range(3):
-            flush.zero_()
-            gpu1.eval_device(d_q.data_ptr(), nq, out.data_ptr(), pb, stream=s_handle)
-        times = []
-        for _ in range(max(3, args.steps // 4)):
-            flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            gpu1.eval_device(d_q.data_ptr(), nq, out.data_ptr(), pb, stream=s_handle)
-            e1.record(stream)
-            times.append((e0, e1))
-        torch.cuda.synchronize(dev)
-        ms = statistics.mean(a.elapsed_time(b) for a, b in times)
-        eb = rel_errors(wl["kernel"], out[:n_sub].cpu().numpy(), ref_np)
-        compare[f"barnes_hut_theta_{theta}"] = {
-            "tree": "dim_split_log 1 (branching 8), leaf 1", "queries_per_s": nq / (ms / 1e3),
-            "ms_per_step": ms, "median_rel_err": float(np.median(eb)),
-            "p99_rel_err": float(np.percentile(eb, 99))}
+    kid = p.kernel
+    R = gpu.info.root_children
+    runs = [(f"stochastic_budget_{b}", gpu,
+             C.params(method=C.STOCHASTIC, kernel=kid, samples_per_subdomain=max(1, b // R),
+                      seed=p.seed), {"tree": "dim_split_log 2 (branching 64), leaf 1",
+                                     "paths_per_query": max(1, b // R) * R})
+            for b in (64, 128, 256, 512, 1024)]
+    runs += [(f"barnes_hut_theta_{th}", gpu1, C.params(method=C.BARNES_HUT, kernel=kid,
+                                                       beta=1.0 / th),
+              {"tree": "dim_split_log 1 (branching 8), leaf 1"}) for th in (0.3, 0.5, 0.8)]
+    for name, g, pr, extra in runs:
+        ms = statistics.mean(timed_device(
+            lambda: g.eval_device(d_q.data_ptr(), nq, out.data_ptr(), pr, stream=s_handle),
+            stream, flush, 3, max(3, args.steps // 4)))
+        eb = rel_errors(wl["kernel"], out[:n_sub].cpu().numpy(), ref)
+        compare[name] = dict(extra, queries_per_s=nq / (ms / 1e3), ms_per_step=ms,
+                             median_rel_err=float(np.median(eb)),
+                             p99_rel_err=float(np.percentile(eb, 99)))
     gpu1.check(s_handle)
     return accuracy, compare
 
@@ -548,6 +689,11 @@ def run_ref(t, wl, kid, q, samples):
 
 
 def run_reference(args, wl):
+    """The reference's own CPU plugin (src/sbh.cpp, compiled unmodified in
+    oracle/_ref) on the same workload: its std::thread pool over all host
+    threads, a bounded query sample per step.  Nothing of this library is
+    loaded: the tree, its root-child count (the sampler's budget mapping) and
+    the configuration come from the reference build itself."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return None
@@ -558,12 +704,7 @@ def run_reference(args, wl):
         return {"impl": "reference", "unavailable": "oracle/_ref/libsbh_ref.so is not built"}
     pts, nrm, m, lo, hi, q = make_inputs(wl, 0)
     t = O.RefTree(pts, nrm, m, lo, hi, dim_split_log=wl["dsl"], leaf_size=wl["leaf"])
-    info_children = int((t.dump().parent == 0).sum() - 1) if wl["n"] <= 200000 else None
-    if info_children is None:
-        import sbh_capi as C
-        info_children = C.HostTree(pts, nrm, m, lo, hi, dim_split_log=wl["dsl"],
-                                   leaf_size=wl["leaf"]).info().root_children
-    samples = W.samples_for_budget(wl.get("budget", 1), info_children)
+    samples = W.samples_for_budget(wl.get("budget", 1), t.root_children)
     kid = {"gravity": 0, "wn": 1, "smooth": 2}.get(wl["kernel"])
     cores = O.ref_hardware_concurrency()
     per_step = max(64, args.ref_sample)
@@ -579,11 +720,12 @@ def run_reference(args, wl):
     sample = (f"{per_step} queries per step of the {len(q)}-query workload, "
               f"src/sbh.cpp thread pool ({cores} threads), tree build excluded")
     return {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "impl": "reference", "metric": WORKLOAD_METRIC[wl["name"]], "value": value,
+        "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
-        "config": {"workload": wl["desc"], "samples_per_subdomain": samples},
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generators; the reference publishes no dataset)",
+        "config": workload_config(wl, t.num_nodes, t.root_children, samples),
         "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores,
                          "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
@@ -594,13 +736,34 @@ def run_reference(args, wl):
 # ----------------------------------------------------------------- serving
 
 SERVING_KERNELS = ("gravity", "wn", "smooth")
+SERVING_KID = {"gravity": 0, "wn": 1, "smooth": 2}  # SBH_KERNEL_* (the reference's KernelFuncID)
+SERVING_ALPHA = 100.0
+MATCH_TARGET = 1e-3
+
+# Operating points at matched accuracy (median relative error <= 1e-3 against
+# FP64 brute force, per kernel, on the serving mix): the plain per-call
+# Barnes-Hut's opening angle theta, and for the served path the method and the
+# factor on every request's drawn sample budget (64/256/1024).  Chosen by
+# `python bench.py --workload serving --calibrate` (the largest theta and the
+# smallest budget factor that reach the target; a kernel whose stochastic
+# estimate does not reach it within 16x the budgets is served by Barnes-Hut at
+# its matched theta); every bench run re-measures the errors at these points.
+MATCHED = {
+    "gravity": {"theta": 0.5, "served": "stochastic", "budget_scale": 1.0},
+    "wn": {"theta": 0.3, "served": "stochastic", "budget_scale": 4.0},
+    "smooth": {"theta": 0.1, "served": "barnes_hut", "budget_scale": None},
+}
+CAL_THETAS = (0.8, 0.6, 0.5, 0.4, 0.3, 0.25, 0.2, 0.15, 0.1, 0.07, 0.05)
+CAL_SCALES = (0.25, 0.5, 1.0, 2.0, 4.0, 8.0, 16.0)
 
 
-def serving_setup(C, seed=77, n_trees=32, n_requests=1500):
+def serving_setup(C, seed=77, n_trees=32, n_requests=1500, device_trees=True):
     """32 resident trees (16 3D, 16 2D; Gaussian mixtures, torus, sphere and
     circle surfaces; 10^4..2*10^6 points log-uniform) and a seeded request list:
     tree, kernel (gravity / winding number / smooth distance alpha 100), query
-    count log-uniform in [1, 10^5] uniform in the tree's box, budget 64/256/1024."""
+    count log-uniform in [1, 10^5] uniform in the tree's box, budget 64/256/1024.
+    With device_trees the trees are built on the GPU in both layouts (Octree1 /
+    Quadtree1 for Barnes-Hut, Octree2 / Quadtree2 for the sampler)."""
     import sbh_workloads as W
     rng = np.random.default_rng(seed)
     trees = []
@@ -617,11 +780,13 @@ def serving_setup(C, seed=77, n_trees=32, n_requests=1500):
             pts, nrm, m = (W.gaussian_mixture(n, seed + i, dim=2) if kind == "gauss" else
                            W.circle_points(n, seed + i))
         lo, hi = W.padded_box(pts)
-        # built on the device (sbh_gpu_tree_build; the same trees as a host build)
-        g1 = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=1)
-        g2 = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=2)
-        trees.append(dict(dim=dim, kind=kind, n=n, lo=lo, hi=hi, bh=g1, sbh=g2,
-                          root2=g2.info.root_children))
+        t = dict(dim=dim, kind=kind, n=n, lo=lo, hi=hi, pts=pts, nrm=nrm, m=m)
+        if device_trees:
+            # built on the device (sbh_gpu_tree_build; the same trees as a host build)
+            t["bh"] = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=1)
+            t["sbh"] = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=2)
+            t["root2"] = t["sbh"].info.root_children
+        trees.append(t)
     reqs = []
     for r in range(n_requests):
         ti = int(rng.integers(n_trees))
@@ -634,13 +799,28 @@ def serving_setup(C, seed=77, n_trees=32, n_requests=1500):
     return trees, reqs
 
 
-def serving_params(C, W, t, r, method, theta=0.5):
-    kid = {"gravity": C.GRAVITY, "wn": C.WINDING_NUMBER, "smooth": C.SMOOTH_DIST}[r["kernel"]]
-    alpha = 100.0 if r["kernel"] == "smooth" else None
-    if method == "sbh":
+def request_params(C, W, t, r, method, theta=None, budget_scale=None):
+    """Parameters of request r served by `method` ("stochastic" / "barnes_hut")
+    at the given operating point (default: the matched one of its kernel)."""
+    op = MATCHED[r["kernel"]]
+    kid = SERVING_KID[r["kernel"]]
+    alpha = SERVING_ALPHA if r["kernel"] == "smooth" else None
+    if method == "stochastic":
+        scale = op["budget_scale"] if budget_scale is None else budget_scale
+        scale = 1.0 if scale is None else scale
         return C.params(method=C.STOCHASTIC, kernel=kid, alpha=alpha, seed=r["nq"],
-                        samples_per_subdomain=W.samples_for_budget(r["budget"], t["root2"]))
-    return C.params(method=C.BARNES_HUT, kernel=kid, alpha=alpha, beta=1.0 / theta)
+                        samples_per_subdomain=W.samples_for_budget(
+                            int(round(r["budget"] * scale)), t["root2"]))
+    th = op["theta"] if theta is None else theta
+    return C.params(method=C.BARNES_HUT, kernel=kid, alpha=alpha, beta=1.0 / th)
+
+
+def served_method(r):
+    return MATCHED[r["kernel"]]["served"]
+
+
+def tree_for(t, method):
+    return t["sbh"] if method == "stochastic" else t["bh"]
 
 
 def wait_until(t0, at):
@@ -651,8 +831,10 @@ def wait_until(t0, at):
         time.sleep(d if d > 2e-3 else 0)
 
 
-def drive_plain(C, W, trees, reqs, gpus, arrivals, method="bh"):
-    """The reference's usage: one blocking call per request, in arrival order."""
+def drive_plain(C, W, trees, reqs, arrivals):
+    """The reference's usage: one blocking per-call Barnes-Hut evaluation per
+    request (host buffers, copies inside the call), in arrival order, at the
+    kernel's matched theta."""
     outs = []
     lat = []
     t0 = time.perf_counter()
@@ -660,26 +842,27 @@ def drive_plain(C, W, trees, reqs, gpus, arrivals, method="bh"):
         wait_until(t0, at)
         t = trees[r["tree"]]
         out = np.empty(r["nq"], np.float32)
-        g = gpus[r["tree"]]
-        g.eval_host_ptr(r["q"].ctypes.data, r["nq"], out.ctypes.data,
-                        serving_params(C, W, t, r, method))
+        t["bh"].eval_host_ptr(r["q"].ctypes.data, r["nq"], out.ctypes.data,
+                              request_params(C, W, t, r, "barnes_hut"))
         lat.append((time.perf_counter() - t0 - at) * 1e3)
         outs.append(out)
     return time.perf_counter() - t0, np.array(lat), outs
 
 
-def drive_served(C, W, trees, reqs, server, ids, arrivals, method):
+def drive_served(C, W, trees, reqs, server, ids, arrivals, method=None):
+    """Requests submitted to the server at their arrival times (host buffers);
+    method None: each kernel's matched served method."""
     handles = [None] * len(reqs)
     lateness = np.zeros(len(reqs))
 
     def submitter():
-        t0s = t0
         for k, (r, at) in enumerate(zip(reqs, arrivals)):
-            wait_until(t0s, at)
-            lateness[k] = (time.perf_counter() - t0s - at) * 1e3
+            wait_until(t0, at)
+            lateness[k] = (time.perf_counter() - t0 - at) * 1e3
             t = trees[r["tree"]]
-            handles[k] = server.submit(ids[(r["tree"], method)], r["q"],
-                                       serving_params(C, W, t, r, method))
+            mth = method or served_method(r)
+            handles[k] = server.submit(ids[(r["tree"], mth)], r["q"],
+                                       request_params(C, W, t, r, mth))
 
     t0 = time.perf_counter()
     th = threading.Thread(target=submitter)
@@ -692,121 +875,301 @@ def drive_served(C, W, trees, reqs, server, ids, arrivals, method):
     return time.perf_counter() - t0, np.array(lat), [h.results for h in handles]
 
 
-def serving_errors(C, trees, reqs, gpus_bf, outs, pick):
-    """Median relative error per kernel against float32 brute force with compensated
-    sums, on the first 2048 queries of each picked request.  Gravity: |e|/|ref|;
-    winding number: |e|/max(|ref|, 1); smooth distance: the error of
-    D = -log(S)/alpha, the distance the sum S stands for (a non-positive estimate
-    of S counts as an infinite error)."""
-    errs = {k: [] for k in SERVING_KERNELS}
+def serving_error(kernel, est, ref):
+    """Relative error against FP64: gravity |e|/|ref|; winding number
+    |e|/max(|ref|, 1); smooth distance the error of D = -log(S)/alpha, the
+    distance the sum S stands for (a non-positive estimate of S counts as an
+    infinite error)."""
+    est = est.astype(np.float64)
+    if kernel == "wn":
+        return np.abs(est - ref) / np.maximum(np.abs(ref), 1.0)
+    if kernel == "gravity":
+        return np.abs(est - ref) / np.abs(ref)
+    ok = ref > 0
+    d_ref = -np.log(ref[ok]) / SERVING_ALPHA
+    with np.errstate(divide="ignore", invalid="ignore"):
+        d_est = np.where(est[ok] > 0, -np.log(np.maximum(est[ok], 1e-300)) / SERVING_ALPHA,
+                         np.inf)
+    return np.abs(d_est - d_ref) / np.abs(d_ref)
+
+
+def serving_references(trees, reqs, per_kernel=30, n_max=1024, seed=5):
+    """FP64 brute-force values (the oracle's GPU FP64 kernel) for the first
+    n_max queries of `per_kernel` seeded requests of each kernel."""
+    rng = np.random.default_rng(seed)
+    pick = []
+    for kern in SERVING_KERNELS:
+        idx = [k for k, r in enumerate(reqs) if r["kernel"] == kern]
+        pick += [int(k) for k in rng.permutation(idx)[:per_kernel]]
+    refs = {}
     for k in pick:
         r = reqs[k]
-        n = min(r["nq"], 2048)
-        kid = {"gravity": C.GRAVITY, "wn": C.WINDING_NUMBER, "smooth": C.SMOOTH_DIST}[r["kernel"]]
-        alpha = 100.0 if r["kernel"] == "smooth" else None
-        ref, _ = gpus_bf[r["tree"]].eval(r["q"][:n], C.params(method=C.BRUTE_FORCE, kernel=kid,
-                                                               alpha=alpha))
-        est = outs[k][:n].astype(np.float64)
-        ref = ref.astype(np.float64)
-        if r["kernel"] == "wn":
-            e = np.abs(est - ref) / np.maximum(np.abs(ref), 1.0)
-        elif r["kernel"] == "gravity":
-            e = np.abs(est - ref) / np.abs(ref)
-        else:
-            ok = ref > 0
-            d_ref = -np.log(ref[ok]) / 100.0
-            with np.errstate(divide="ignore", invalid="ignore"):
-                d_est = np.where(est[ok] > 0, -np.log(np.maximum(est[ok], 1e-300)) / 100.0, np.inf)
-            e = np.abs(d_est - d_ref) / np.abs(d_ref)
-        errs[r["kernel"]].append(e)
-    return {k: (float(np.median(np.concatenate(v))) if v else None) for k, v in errs.items()}
-
-
-def serving_tuning(C, W, trees, reqs, gpus, n=256):
-    """Batch schedule for the server, chosen by the autotuner on a representative
-    batch: the first `n` requests of the stream, each once as stochastic BH and
-    once as Barnes-Hut (untimed)."""
-    import torch
-    entries, keep = [], []
-    for r in reqs[:n]:
         t = trees[r["tree"]]
+        n = min(r["nq"], n_max)
+        refs[k] = fp64_reference(t["pts"], t["nrm"], t["m"], r["kernel"],
+                                 np.ascontiguousarray(r["q"][:n]),
+                                 alpha=SERVING_ALPHA if r["kernel"] == "smooth" else 1.0)
+    return refs
+
+
+def median_errors(C, W, trees, reqs, refs, method, kernel, **op):
+    """Median error of `method` at an operating point over the picked requests
+    of one kernel (blocking calls on the first queries of each)."""
+    errs = []
+    for k, ref in refs.items():
+        r = reqs[k]
+        if r["kernel"] != kernel:
+            continue
+        t = trees[r["tree"]]
+        v, _ = tree_for(t, method).eval(r["q"][:len(ref)],
+                                        request_params(C, W, t, r, method, **op))
+        errs.append(serving_error(kernel, v, ref))
+    e = np.concatenate(errs)
+    return float(np.median(e)), float(np.percentile(e, 99))
+
+
+def serving_calibrate(C, W, trees, reqs, refs):
+    """The calibration ladders: median error per kernel for every plain theta
+    and every budget factor of the stochastic method."""
+    out = {}
+    for kern in SERVING_KERNELS:
+        rows = {"barnes_hut": {}, "stochastic": {}}
+        for th in CAL_THETAS:
+            rows["barnes_hut"][th] = median_errors(C, W, trees, reqs, refs, "barnes_hut", kern,
+                                                   theta=th)
+        for sc in CAL_SCALES:
+            rows["stochastic"][sc] = median_errors(C, W, trees, reqs, refs, "stochastic", kern,
+                                                   budget_scale=sc)
+        ok_th = [th for th in CAL_THETAS if rows["barnes_hut"][th][0] <= MATCH_TARGET]
+        ok_sc = [sc for sc in CAL_SCALES if rows["stochastic"][sc][0] <= MATCH_TARGET]
+        out[kern] = {"ladders": {m: {str(k): v for k, v in d.items()} for m, d in rows.items()},
+                     "theta": max(ok_th) if ok_th else None,
+                     "budget_scale": min(ok_sc) if ok_sc else None}
+    return out
+
+
+def device_batch(C, W, torch, trees, reqs, method_of):
+    """Batch entries for every request with its queries resident on the device."""
+    entries, keep = [], []
+    for r in reqs:
+        t = trees[r["tree"]]
+        mth = method_of(r)
         dq = torch.from_numpy(np.ascontiguousarray(r["q"].T)).cuda()
-        for method, g in (("sbh", t["sbh"]), ("bh", t["bh"])):
-            out = torch.empty(r["nq"], dtype=torch.float32, device="cuda")
-            entries.append((g, serving_params(C, W, t, r, method), dq.data_ptr(), r["nq"],
-                            out.data_ptr(), 0, 0))
-            keep.append(out)
-        keep.append(dq)
-    best, best_ms, start_ms = C.batch_autotune(entries, stream=0, repeats=2)
-    torch.cuda.synchronize()
-    return best, {"tuning": best.as_dict(), "tuned_ms": best_ms, "default_ms": start_ms,
-                  "batch": f"first {n} requests, each as stochastic BH and as Barnes-Hut"}
+        out = torch.empty(r["nq"], dtype=torch.float32, device="cuda")
+        entries.append((tree_for(t, mth), request_params(C, W, t, r, mth), dq.data_ptr(),
+                        r["nq"], out.data_ptr(), 0, 0))
+        keep += [dq, out]
+    return entries, keep
 
 
 def run_serving(args):
+    import torch
+
     import sbh_capi as C
     import sbh_workloads as W
     t_setup = time.perf_counter()
     trees, reqs = serving_setup(C)
-    gpus = {i: t["bh"] for i, t in enumerate(trees)}
-    tuning, tune_info = serving_tuning(C, W, trees, reqs, gpus)
+    refs = serving_references(trees, reqs)
+    if args.calibrate:
+        return {"calibration": serving_calibrate(C, W, trees, reqs, refs),
+                "target": MATCH_TARGET, "requests_per_kernel": len(refs) // 3}
+    total_q = sum(r["nq"] for r in reqs)
+
+    # Accuracy at the matched operating points (and of the stochastic method on
+    # every kernel at its configured budgets, for reference).
+    acc = {}
+    for kern in SERVING_KERNELS:
+        op = MATCHED[kern]
+        acc[kern] = {
+            "plain_barnes_hut": dict(zip(("median_rel_err", "p99_rel_err"), median_errors(
+                C, W, trees, reqs, refs, "barnes_hut", kern)), theta=op["theta"]),
+            "served": dict(zip(("median_rel_err", "p99_rel_err"), median_errors(
+                C, W, trees, reqs, refs, op["served"], kern)), method=op["served"],
+                budget_scale=op["budget_scale"]),
+            "stochastic_at_drawn_budgets": dict(zip(("median_rel_err", "p99_rel_err"),
+                                                    median_errors(C, W, trees, reqs, refs,
+                                                                  "stochastic", kern,
+                                                                  budget_scale=1.0))),
+        }
+    matched = all(max(a["plain_barnes_hut"]["median_rel_err"], a["served"]["median_rel_err"])
+                  <= MATCH_TARGET for a in acc.values())
+
+    # Batch schedule for the served path, autotuned on the first 256 requests (untimed).
+    entries, keep = device_batch(C, W, torch, trees, reqs[:256], served_method)
+    tuning, best_ms, start_ms = C.batch_autotune(entries, stream=0, repeats=2)
+    torch.cuda.synchronize()
+    del entries, keep
+
+    # value: the whole request stream as one batched evaluation with every
+    # request's queries resident in HBM, at the matched operating points.
+    entries, keep = device_batch(C, W, torch, trees, reqs, served_method)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    with ClockSampler(0) as clocks:
+        dev_ms = timed_device(lambda: C.eval_batch(entries, stream=stream.cuda_stream), stream,
+                              flush, args.warmup, args.steps)
+    del entries, keep
+    dev_total_ms = float(sum(dev_ms))
+
     server = C.Server(slots=3, slot_queries=1 << 20, max_requests_per_batch=4096, tuning=tuning)
     ids = {}
     for i, t in enumerate(trees):
-        ids[(i, "sbh")] = server.add_tree(t["sbh"])
-        ids[(i, "bh")] = server.add_tree(t["bh"])
+        ids[(i, "stochastic")] = server.add_tree(t["sbh"])
+        ids[(i, "barnes_hut")] = server.add_tree(t["bh"])
     setup_s = time.perf_counter() - t_setup
-    total_q = sum(r["nq"] for r in reqs)
-    # Warm up every path once on a slice of the stream.
+    # Warm-up of every path on a slice of the stream.
     warm = reqs[:50]
-    drive_plain(C, W, trees, warm, gpus, np.zeros(len(warm)))
-    drive_served(C, W, trees, warm, server, ids, np.zeros(len(warm)), "bh")
-    drive_served(C, W, trees, warm, server, ids, np.zeros(len(warm)), "sbh")
-    # Capacity of the plain path: every request queued at t = 0 (the first pass
-    # also grows every tree's cached workspace to its largest request).
-    drive_plain(C, W, trees, reqs, gpus, np.zeros(len(reqs)))
-    mk, _, plain_outs = drive_plain(C, W, trees, reqs, gpus, np.zeros(len(reqs)))
-    plain_rps = len(reqs) / mk
+    drive_plain(C, W, trees, warm, np.zeros(len(warm)))
+    drive_served(C, W, trees, warm, server, ids, np.zeros(len(warm)))
+    # Plain per-call capacity: every request queued at t = 0 (the first pass also
+    # grows every tree's cached workspace to its largest request).
+    drive_plain(C, W, trees, reqs, np.zeros(len(reqs)))
+    plain_mk, plain_lat, _ = drive_plain(C, W, trees, reqs, np.zeros(len(reqs)))
+    plain_rps = len(reqs) / plain_mk
+    # Served capacity (e2e): the same stream submitted at t = 0, host buffers.
+    served_mk, served_lat, _ = drive_served(C, W, trees, reqs, server, ids, np.zeros(len(reqs)))
+    served_bh_mk, _, _ = drive_served(C, W, trees, reqs, server, ids, np.zeros(len(reqs)),
+                                      method="barnes_hut")
+    rates = {}
     rng = np.random.default_rng(5)
-    pick = [k for k in rng.permutation(len(reqs))[:90]]
-    results = {"plain_bh_capacity": {"queries_per_s": total_q / mk, "requests_per_s": plain_rps,
-                                     "median_rel_err": serving_errors(C, trees, reqs, gpus,
-                                                                      plain_outs, pick)}}
-    sampler = ClockSampler(0)
-    sampler.__enter__()
-    for factor in (0.5, 1.0, 2.0, 8.0):
+    for factor in (0.5, 1.0, 2.0):
         rate = factor * plain_rps
         gaps = rng.exponential(1.0 / rate, len(reqs))
         arrivals = np.cumsum(gaps) - gaps[0]
         row = {"arrival_rate_rps": rate}
-        for name, fn in (("plain_bh", lambda: drive_plain(C, W, trees, reqs, gpus, arrivals)),
-                         ("served_bh", lambda: drive_served(C, W, trees, reqs, server, ids,
-                                                            arrivals, "bh")),
-                         ("served_sbh", lambda: drive_served(C, W, trees, reqs, server, ids,
-                                                             arrivals, "sbh"))):
-            mk, lat, outs = fn()
+        for name, fn in (("plain_barnes_hut", lambda: drive_plain(C, W, trees, reqs, arrivals)),
+                         ("served", lambda: drive_served(C, W, trees, reqs, server, ids,
+                                                         arrivals))):
+            mk, lat, _ = fn()
             row[name] = {"queries_per_s": total_q / mk, "p50_ms": float(np.percentile(lat, 50)),
                          "p99_ms": float(np.percentile(lat, 99)), "makespan_s": mk}
-            if factor == 8.0:
-                row[name]["median_rel_err"] = serving_errors(C, trees, reqs, gpus, outs, pick)
-        results[f"rate_x{factor}"] = row
-    sampler.__exit__(None, None, None)
+        rates[f"rate_x{factor}"] = row
     stats = server.stats()
     server.close()
-    hi = results["rate_x8.0"]
+    served_qps = total_q / served_mk
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        if O.ref_available():
+            cq, cs, cn, _ = reference_serving_sample(trees, reqs, args.cpu_seconds)
+            cores = O.ref_hardware_concurrency()
+            cpu = {"value": cq / cs, "unit": "queries/s", "cores": cores, "kind": "reference",
+                   "sample": f"the first {cn} requests of the stream ({int(cq)} queries), "
+                             f"src/sbh.cpp evalBarnesHut at each kernel's matched theta, its "
+                             f"thread pool ({cores} threads), {cs:.1f} s"}
+    plain_qps = total_q / plain_mk
     return {
-        "metric": METRIC, "value": hi["served_sbh"]["queries_per_s"], "unit": "queries/s",
-        "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": hi["served_sbh"]["makespan_s"] * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded generators)",
-        "config": {"workload": "serving: 32 resident trees (16 3D, 16 2D), 1500 Poisson requests, "
-                               "gravity / winding number / smooth distance (alpha 100), 1..1e5 "
-                               "queries log-uniform, budget 64/256/1024; served SBH and BH vs "
-                               "plain per-call BH (theta 0.5)",
-                   "requests": len(reqs), "queries": total_q, "setup_s": setup_s,
-                   "server": {"slots": 3, "slot_queries": 1 << 20}},
-        "serving": results, "server_stats": stats, "clocks": sampler.summary(),
-        "autotune": tune_info,
+        "metric": METRIC, "value": total_q / (dev_total_ms / args.steps / 1e3),
+        "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generators; the reference publishes no dataset)",
+        "config": serving_config(len(reqs), total_q),
+        "e2e": {"value": served_qps, "unit": "queries/s",
+                "h2d_bytes_per_step": sum(r["nq"] * 4 * trees[r["tree"]]["dim"] for r in reqs),
+                "d2h_bytes_per_step": total_q * 4, "ms_per_step": served_mk * 1e3,
+                "path": "sbh_server_submit / sbh_server_wait (C ABI) with host buffers, every "
+                        "request of the stream submitted at t = 0",
+                "p50_ms": float(np.percentile(served_lat, 50)),
+                "p99_ms": float(np.percentile(served_lat, 99))},
+        "served_over_plain": served_qps / plain_qps,
+        "plain_barnes_hut": {"queries_per_s": plain_qps, "requests_per_s": plain_rps,
+                             "p50_ms": float(np.percentile(plain_lat, 50)),
+                             "p99_ms": float(np.percentile(plain_lat, 99)),
+                             "path": "one blocking sbh_eval per request (host buffers), "
+                                     "Barnes-Hut at each kernel's matched theta"},
+        "served_barnes_hut_only": {"queries_per_s": total_q / served_bh_mk},
+        "matched": {"target_median_rel_err": MATCH_TARGET, "all_within_target": matched,
+                    "operating_points": MATCHED, "accuracy": acc,
+                    "reference": "FP64 brute force on the GPU (the oracle's libsbh_bf64.so), "
+                                 "first 1,024 queries of 30 seeded requests per kernel"},
+        "latency_at_rates": rates,
+        "server_stats": stats, "clocks": clocks.summary(),
+        "autotune": {"tuning": tuning.as_dict(), "tuned_ms": best_ms, "default_ms": start_ms},
+        "setup_s": setup_s,
+        "cpu_baseline": cpu,
+        "gpu_launches": None,
+    }
+
+
+def serving_config(n_requests, total_q):
+    return {"workload": "serving: 32 resident trees (16 3D, 16 2D; Gaussian mixtures, torus, "
+                        "sphere and circle surfaces; 1e4..2e6 points), 1500 seeded requests, "
+                        "gravity / winding number / smooth distance (alpha 100), 1..1e5 "
+                        "queries log-uniform, budgets 64/256/1024 scaled per kernel to matched "
+                        "accuracy; served (continuous batching) vs plain per-call Barnes-Hut, "
+                        "both at median relative error <= 1e-3 vs FP64",
+            "requests": n_requests, "queries": total_q,
+            "server": {"slots": 3, "slot_queries": 1 << 20},
+            "l2": "512 MiB buffer written between timed batch steps"}
+
+
+def reference_serving_sample(trees, reqs, budget_s, start=0, ref_trees=None):
+    """The reference's CPU plugin (src/sbh.cpp evalBarnesHut, compiled unmodified
+    in oracle/_ref, its own thread pool) on consecutive requests of the stream
+    from `start`, each at its kernel's matched theta, until `budget_s` seconds
+    of evaluation: (queries, seconds, requests, next start).  Reference trees
+    (Octree1 / Quadtree1, alpha 100) are built on first use; builds are not
+    timed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ref_trees = {} if ref_trees is None else ref_trees
+    nq = secs = 0.0
+    done = 0
+    k = start
+    while secs < budget_s and done < len(reqs):
+        r = reqs[k % len(reqs)]
+        t = trees[r["tree"]]
+        if r["tree"] not in ref_trees:
+            ref_trees[r["tree"]] = O.RefTree(t["pts"], t["nrm"], t["m"], t["lo"], t["hi"],
+                                             alpha=SERVING_ALPHA, dim_split_log=1)
+        _, s = ref_trees[r["tree"]].plugin_bh(SERVING_KID[r["kernel"]],
+                                              np.ascontiguousarray(r["q"]),
+                                              1.0 / MATCHED[r["kernel"]]["theta"])
+        nq += r["nq"]
+        secs += s
+        done += 1
+        k += 1
+    return nq, secs, done, k
+
+
+def run_reference_serving(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libsbh_ref.so is not built"}
+    trees, reqs = serving_setup(None, device_trees=False)
+    ref_trees = {}
+    k = 0
+    for _ in range(args.warmup):
+        _, _, _, k = reference_serving_sample(trees, reqs, 0.2, k, ref_trees)
+    tq = ts = 0.0
+    nreq = 0
+    for _ in range(args.steps):
+        q, s, n, k = reference_serving_sample(trees, reqs, args.ref_step_seconds, k, ref_trees)
+        tq += q
+        ts += s
+        nreq += n
+    value = tq / ts
+    cores = O.ref_hardware_concurrency()
+    sample = (f"{nreq} consecutive requests of the 1500-request stream ({int(tq)} queries), "
+              f"src/sbh.cpp evalBarnesHut per request at each kernel's matched theta, its thread "
+              f"pool ({cores} threads); tree builds excluded")
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ts / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generators; the reference publishes no dataset)",
+        "config": serving_config(len(reqs), sum(r["nq"] for r in reqs)),
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
     }
 
 
@@ -1051,7 +1414,7 @@ def main():
     ap.add_argument("--workload",
                     choices=sorted(WORKLOADS) + ["serving", "batching", "differentiation",
                                                  "tree_build"],
-                    default="sbh_wn")
+                    default="serving")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -1060,6 +1423,12 @@ def main():
     ap.add_argument("--nq", type=int, default=0, help="override the query count (profiling)")
     ap.add_argument("--budget", type=int, default=0,
                     help="override the sampled paths per query of a stochastic workload")
+    ap.add_argument("--stage-leaves", action="store_true",
+                    help="Barnes-Hut workloads: copy accepted leaves' points to shared memory "
+                         "with bulk asynchronous copies (SBH_FLAG_STAGE_LEAVES)")
+    ap.add_argument("--calibrate", action="store_true",
+                    help="serving: print the accuracy ladders the matched operating points "
+                         "are chosen from, instead of timing")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -1068,8 +1437,13 @@ def main():
     if args.workload in systems and args.impl == "ours":
         print(json.dumps(systems[args.workload](args)), flush=True)
         return
+    if args.workload == "serving":
+        out = run_reference_serving(args)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
     if args.workload in systems:
-        ap.error("--impl reference runs the default workloads only")
+        ap.error("--impl reference runs the serving and single-configuration workloads only")
     wl = dict(WORKLOADS[args.workload])
     wl["name"] = args.workload
     wl["resized"] = bool(args.nq or args.budget)

@@ -66,6 +66,13 @@ typedef enum sbh_method {
 
 /* sbh_params.flags */
 #define SBH_FLAG_KEEP_ORDER 0x1u /* evaluate queries in the given order (no spatial sort) */
+/* Barnes-Hut (SBH_METHOD_BARNES_HUT, single calls): copy the points of every
+ * accepted leaf that holds several of them (leaf sizes above 1) into the warp's
+ * shared memory with one bulk asynchronous copy (cp.async.bulk, no multicast)
+ * and evaluate them from there, instead of one load per point from L1/L2.
+ * Results are identical; it is a schedule choice, measured against the default
+ * on the leaf-size-8 workload. */
+#define SBH_FLAG_STAGE_LEAVES 0x2u
 
 typedef struct sbh_params {
   int32_t method;                /* sbh_method */
@@ -311,10 +318,15 @@ void sbh_server_destroy(sbh_server* server);
  * under memory pressure at any moment), or code whose device memory belongs to
  * another allocator's budget, such as a framework's caching allocator.
  * Limits and rules:
- *   - at most SBH_STATIC_SCRATCH_MAX_QUERIES queries per call; larger counts
- *     return SBH_ERR_INVALID_ARGUMENT (split the batch);
- *   - the first call on a device looks up the array's device address with that
- *     device current; make that first call before any stream capture begins;
+ *   - calls that order their queries (Barnes-Hut and stochastic without
+ *     SBH_FLAG_KEEP_ORDER) take at most SBH_STATIC_SCRATCH_MAX_QUERIES queries;
+ *     larger counts return SBH_ERR_INVALID_ARGUMENT (split the batch).  Brute
+ *     force, warp-vote Barnes-Hut and SBH_FLAG_KEEP_ORDER calls use no scratch
+ *     and take any count;
+ *   - every call looks up the array's device address with the tree's device
+ *     current; the first call on a device also loads the library's device code
+ *     there, so make it before any stream capture begins.  Trees do not survive
+ *     a device reset, so neither does anything this entry point works on;
  *   - all calls share the one array and it keeps the previous call's contents
  *     (each call re-initialises what it reads), so calls that overlap on the
  *     GPU -- on different streams or from different threads -- race: order

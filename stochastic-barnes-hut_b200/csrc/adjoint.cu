@@ -54,22 +54,13 @@ __global__ void __launch_bounds__(AD_THREADS)
                     int* __restrict__ contribs, int* status) {
   using V = typename A::V;
   extern __shared__ float s_mem[];
-  const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const SbhWarpSmem<V> ws =
-      sbh_carve<V>(s_mem + (size_t)warp * sbh_warp_words<V>(t.root_children), t.root_children);
+  const SbhWarpSmem<V> ws = sbh_carve<V>(s_mem + (size_t)warp * sbh_warp_words<V>());
+  const long long units = (nq + 31) / 32;
   const long long stride = (long long)gridDim.x * AD_WARPS;
-  for (long long slot = (long long)blockIdx.x * AD_WARPS + warp; slot < nq; slot += stride) {
-    const long long qi = order ? (long long)__ldg(order + slot) : slot;
-    V r;
-    int c;
-    sbh_query<DIM, K, A>(t, load_query<DIM>(qsoa, nq, qi), qi, samples, seed, kp, ws, status, r,
-                         c);
-    if (lane == 0) {
-      A::store(out, grads, nq, qi, r, kp);
-      if (contribs) contribs[qi] = c;
-    }
-  }
+  for (long long u = (long long)blockIdx.x * AD_WARPS + warp; u < units; u += stride)
+    sbh_warp_task<DIM, K, A>(t, qsoa, nq, order, u * 32, min(nq, u * 32 + 32), 0, samples, seed,
+                             kp, ws, status, out, contribs, nullptr, grads);
 }
 
 // ----------------------------------------------------------- brute force ---
@@ -179,14 +170,14 @@ cudaError_t launch_policy(const DevTree& t, int method, const float* q, long lon
     return cudaGetLastError();
   }
   using V = typename A::V;
-  const size_t smem = (size_t)AD_WARPS * sbh_warp_words<V>(t.root_children) * sizeof(float);
+  const size_t smem = (size_t)AD_WARPS * sbh_warp_words<V>() * sizeof(float);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(sbh_grad_kernel<DIM, K, A>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  long long blocks = (nq + AD_WARPS - 1) / AD_WARPS;
-  const long long cap = (long long)sm_count * 32;
+  long long blocks = ((nq + 31) / 32 + AD_WARPS - 1) / AD_WARPS;
+  const long long cap = (long long)sm_count * 256;
   if (blocks > cap) blocks = cap;
   sbh_grad_kernel<DIM, K, A><<<(unsigned)blocks, AD_THREADS, smem, stream>>>(
       t, q, nq, order, samples, seed, kp, out, grads, contribs, status);
@@ -196,8 +187,9 @@ cudaError_t launch_policy(const DevTree& t, int method, const float* q, long lon
 }  // namespace
 
 size_t gradient_smem_bytes(const DevTree& t, int kernel) {
-  const size_t words = kernel == kSmoothDist ? sbh_warp_words<LseValue>(t.root_children)
-                                             : sbh_warp_words<GradValue>(t.root_children);
+  (void)t;
+  const size_t words = kernel == kSmoothDist ? sbh_warp_words<LseValue>()
+                                             : sbh_warp_words<GradValue>();
   return (size_t)AD_WARPS * words * sizeof(float);
 }
 

@@ -21,18 +21,32 @@ namespace {
 constexpr int BH_THREADS = 128;
 constexpr int BH_WARPS = BH_THREADS / 32;
 
-// Each warp takes `group` consecutive (sorted) queries, one per lane.
-template <int DIM, int K, bool VOTE>
+template <bool STAGE>
+__host__ __device__ constexpr size_t warp_smem_bytes(int stack_cap) {
+  return ((STAGE ? sizeof(BhLeafStage) : 0) + (size_t)stack_cap * sizeof(BhStackEntry) + 15) /
+         16 * 16;
+}
+
+// Each warp takes `group` consecutive (sorted) queries, one per lane.  With
+// STAGE each warp's shared memory starts with its leaf stage (BhLeafStage),
+// then its stack.
+template <int DIM, int K, bool VOTE, bool STAGE>
 __global__ void __launch_bounds__(BH_THREADS)
     barnes_hut_kernel(DevTree t, const float* __restrict__ qsoa, long long nq,
                       const int* __restrict__ order, float beta, KParams kp,
                       float* __restrict__ out, int* __restrict__ contribs, int* status,
                       int stack_cap, int group) {
-  extern __shared__ BhStackEntry s_stack[];
+  extern __shared__ float4 s_bh[];
   const int warp = threadIdx.x >> 5;
   const long long slot0 = ((long long)blockIdx.x * BH_WARPS + warp) * group;
-  bh_warp_task<DIM, K, VOTE>(t, qsoa, nq, order, slot0, min(slot0 + group, nq), beta, kp, out,
-                             contribs, status, s_stack + warp * stack_cap, stack_cap, nullptr);
+  const size_t warp_bytes = warp_smem_bytes<STAGE>(stack_cap);
+  char* base = reinterpret_cast<char*>(s_bh) + warp * warp_bytes;
+  BhLeafStage* stage = STAGE ? reinterpret_cast<BhLeafStage*>(base) : nullptr;
+  BhStackEntry* stk = reinterpret_cast<BhStackEntry*>(base + (STAGE ? sizeof(BhLeafStage) : 0));
+  bh_warp_task<DIM, K, VOTE, SumF<DIM, K>, STAGE>(t, qsoa, nq, order, slot0,
+                                                  min(slot0 + group, nq), beta, kp, out,
+                                                  contribs, status, stk, stack_cap, nullptr,
+                                                  nullptr, stage);
 }
 
 // Queries per warp.  A warp's walk covers the union of its lanes' opened sets
@@ -49,16 +63,21 @@ int queries_per_warp(long long nq, bool vote, int sm_count) {
   return g;
 }
 
-template <int DIM, int K, bool VOTE>
+template <int DIM, int K, bool VOTE, bool STAGE>
 cudaError_t launch_bh(const DevTree& t, const float* q, long long nq, const int* order, float beta,
                       const KParams& kp, float* out, int* contribs, int* status,
                       cudaStream_t stream, int sm_count) {
   const int stack_cap = t.depth + 2;
-  const size_t smem = (size_t)BH_WARPS * stack_cap * sizeof(BhStackEntry);
+  const size_t smem = (size_t)BH_WARPS * warp_smem_bytes<STAGE>(stack_cap);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(barnes_hut_kernel<DIM, K, VOTE, STAGE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
   const int group = queries_per_warp(nq, VOTE, sm_count);
   const long long warps = (nq + group - 1) / group;
   const long long blocks = (warps + BH_WARPS - 1) / BH_WARPS;
-  barnes_hut_kernel<DIM, K, VOTE><<<(unsigned)blocks, BH_THREADS, smem, stream>>>(
+  barnes_hut_kernel<DIM, K, VOTE, STAGE><<<(unsigned)blocks, BH_THREADS, smem, stream>>>(
       t, q, nq, order, beta, kp, out, contribs, status, stack_cap, group);
   return cudaGetLastError();
 }
@@ -68,14 +87,16 @@ cudaError_t launch_bh(const DevTree& t, const float* q, long long nq, const int*
 cudaError_t launch_barnes_hut(const DevTree& t, int kernel, bool vote, const float* q,
                               long long nq, const int* order, float beta, const KParams& kp,
                               float* out, int* contribs, int* status, cudaStream_t stream,
-                              int sm_count) {
+                              int sm_count, bool stage_leaves) {
   if (nq <= 0) return cudaSuccess;
-#define SBH_BH_CASE(D, K)                                                                   \
-  if (t.dim == D && kernel == K)                                                            \
-    return vote ? launch_bh<D, K, true>(t, q, nq, order, beta, kp, out, contribs, status,   \
-                                        stream, sm_count)                                   \
-                : launch_bh<D, K, false>(t, q, nq, order, beta, kp, out, contribs, status,  \
-                                         stream, sm_count);
+#define SBH_BH_CASE(D, K)                                                                      \
+  if (t.dim == D && kernel == K)                                                               \
+    return vote           ? launch_bh<D, K, true, false>(t, q, nq, order, beta, kp, out,       \
+                                                         contribs, status, stream, sm_count)   \
+           : stage_leaves ? launch_bh<D, K, false, true>(t, q, nq, order, beta, kp, out,       \
+                                                         contribs, status, stream, sm_count)   \
+                          : launch_bh<D, K, false, false>(t, q, nq, order, beta, kp, out,      \
+                                                          contribs, status, stream, sm_count);
   SBH_BH_CASE(3, kGravity)
   SBH_BH_CASE(3, kWindingNumber)
   SBH_BH_CASE(3, kSmoothDist)

@@ -191,22 +191,12 @@ __device__ __forceinline__ void run_bh(const DevTree& t, const BatchItem& it, lo
 template <int DIM, int K>
 __device__ __forceinline__ void run_sbh(const DevTree& t, const BatchItem& it, long long u,
                                         const int* ord, float* scratch, int* status) {
-  const int lane = threadIdx.x & 31;
-  const SbhWarpSmem<float> ws = sbh_carve<float>(scratch, t.root_children);
+  const SbhWarpSmem<float> ws = sbh_carve<float>(scratch);
   const long long s0 = u * it.unit_queries;
   const long long s1 = min(it.nq, s0 + it.unit_queries);
-  for (long long s = s0; s < s1; s++) {
-    const long long qi = ord ? (long long)__ldg(ord + s) : s;
-    const float3 q = load_query<DIM>(it.q, it.nq, qi);
-    float r;
-    int c;
-    sbh_query<DIM, K>(t, q, it.query_base + qi, it.samples, it.seed, it.kp, ws, status, r, c);
-    if (lane == 0) {
-      if (it.self_mass) r = rsub(r, self_term<DIM, K>(q, __ldg(it.self_mass + qi), it.kp));
-      it.out[qi] = r;
-      if (it.contribs) it.contribs[qi] = c;
-    }
-  }
+  for (long long s = s0; s < s1; s += 32)
+    sbh_warp_task<DIM, K>(t, it.q, it.nq, ord, s, min(s1, s + 32), it.query_base, it.samples,
+                          it.seed, it.kp, ws, status, it.out, it.contribs, it.self_mass);
 }
 
 template <int DIM, int K>
@@ -309,7 +299,8 @@ __global__ void __launch_bounds__(kEvalThreads, CLASS == kClassSbh  ? 8
 int class_warp_words(int cls, int bh_stack, int sbh_r) {
   int scratch = 0;
   if (cls == kClassBh) scratch = bh_stack * (int)sizeof(BhStackEntry) / 4;
-  if (cls == kClassSbh) scratch = sbh_warp_words<float>(sbh_r);
+  if (cls == kClassSbh) scratch = sbh_warp_words<float>();
+  (void)sbh_r;
   return kTreeWords + kItemWords + (scratch + 3) / 4 * 4;
 }
 

@@ -52,6 +52,7 @@ enum : int {
   kStatusTraversalLimit = 1,  // a traversal exceeded its node-visit bound
   kStatusStackOverflow = 2,   // a traversal stack exceeded the tree depth
   kStatusNullChild = 4,       // containedInChild found no node (reference would crash)
+  kStatusCopyTimeout = 8,     // a bulk copy into shared memory did not complete in time
 };
 
 enum KernelId : int { kGravity = 0, kWindingNumber = 1, kSmoothDist = 2, kPlummer = 3 };
@@ -215,6 +216,52 @@ struct PathRng {
 
 __device__ __forceinline__ void report_status(int* status, int bits) {
   if (status) atomicOr(status, bits);
+}
+
+// ---- bulk asynchronous copies global -> shared (one CTA, no multicast) ------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// The calling thread's arrival, announcing `bytes` of copies that complete the phase.
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Orders this thread's earlier generic accesses of shared memory before later
+// asynchronous-proxy writes (a bulk copy into a buffer that was just read).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// `bytes` (a multiple of 16) from global `src` to shared `dst`, both 16-byte
+// aligned, completing on `bar`.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return done != 0;
+}
+// Waits for the phase of `bar` with parity `parity` to complete, giving up
+// after `limit` polls (each poll may itself suspend for a while); returns false
+// on giving up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int limit) {
+  for (int i = 0; i < limit; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
 }
 
 }  // namespace sbh

@@ -61,7 +61,8 @@ cudaError_t run_eval(sbh_gpu_tree* tree, const sbh_params* p, const float* d_q, 
     case SBH_METHOD_BARNES_HUT_VOTE:
       return sbh::launch_barnes_hut(t, p->kernel, p->method == SBH_METHOD_BARNES_HUT_VOTE, d_q,
                                     nq, order, p->beta, kp, d_out, d_contribs, tree->d_status,
-                                    stream, tree->sm_count);
+                                    stream, tree->sm_count,
+                                    (p->flags & SBH_FLAG_STAGE_LEAVES) != 0);
     case SBH_METHOD_STOCHASTIC:
       return sbh::launch_stochastic(t, p->kernel, d_q, nq, order, p->samples_per_subdomain,
                                     p->seed, kp, d_out, d_contribs, tree->d_status, stream,
@@ -471,23 +472,19 @@ namespace {
 
 constexpr size_t kStaticOrderBytes =
     ((size_t)SBH_STATIC_SCRATCH_MAX_QUERIES * sizeof(int) + 255) / 256 * 256;
-constexpr int kStaticMaxDevices = 64;
-std::mutex g_static_mu;
-void* g_static_addr[kStaticMaxDevices] = {};
+static_assert(sbh::query_sort_workspace_bytes(SBH_STATIC_SCRATCH_MAX_QUERIES) + kStaticOrderBytes <=
+                  sizeof(g_static_scratch),
+              "static scratch smaller than the order and sort workspace it holds");
 
-// Device address of g_static_scratch on the current device `dev`, resolved once
-// per device (the host-side name of a __device__ variable is not a device address).
-int static_scratch_address(int dev, char** out) {
-  if (dev < 0 || dev >= kStaticMaxDevices)
-    return sbh::fail(SBH_ERR_UNSUPPORTED, "device index beyond the static scratch table");
-  std::lock_guard<std::mutex> lock(g_static_mu);
-  if (!g_static_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
-    g_static_addr[dev] = p;
-  }
-  *out = static_cast<char*>(g_static_addr[dev]);
+// Device address of g_static_scratch on the current device.  The host-side
+// name of a __device__ variable is not a device address, so it is looked up on
+// every call (the runtime answers from its module table once the module is
+// loaded): nothing cached here can go stale if the caller resets the device.
+int static_scratch_address(char** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+  *out = static_cast<char*>(p);
   return SBH_OK;
 }
 
@@ -499,22 +496,27 @@ SBH_API int sbh_eval_device_static_scratch(sbh_gpu_tree* tree, const sbh_params*
                                            void* stream_ptr) {
   int st = sbh::check_eval_params(tree, params, nq);
   if (st != SBH_OK) return st;
-  if (nq > (int64_t)SBH_STATIC_SCRATCH_MAX_QUERIES)
+  // Only calls that order their queries (Barnes-Hut and stochastic, without
+  // SBH_FLAG_KEEP_ORDER) use the array, so only they are limited by its size.
+  const bool sorts = wants_sort(params);
+  if (sorts && nq > (int64_t)SBH_STATIC_SCRATCH_MAX_QUERIES)
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT,
-                     "sbh_eval_device_static_scratch takes at most " +
+                     "sbh_eval_device_static_scratch orders at most " +
                          std::to_string((long long)SBH_STATIC_SCRATCH_MAX_QUERIES) +
                          " queries per call; got " + std::to_string((long long)nq));
   if (nq == 0) return sbh::ok();
   if (!d_queries || !d_results)
     return sbh::fail(SBH_ERR_INVALID_ARGUMENT, "queries and results must be non-null");
-  if (sbh::query_sort_workspace_bytes(nq) + kStaticOrderBytes > sizeof(g_static_scratch))
-    return sbh::fail(SBH_ERR_UNSUPPORTED, "static scratch is smaller than the sort workspace");
   DeviceGuard guard(tree->device);
-  char* scratch = nullptr;
-  st = static_scratch_address(tree->device, &scratch);
-  if (st != SBH_OK) return st;
-  int* d_ord = reinterpret_cast<int*>(scratch);
-  void* d_sort = scratch + kStaticOrderBytes;
+  int* d_ord = nullptr;
+  void* d_sort = nullptr;
+  if (sorts) {
+    char* scratch = nullptr;
+    st = static_scratch_address(&scratch);
+    if (st != SBH_OK) return st;
+    d_ord = reinterpret_cast<int*>(scratch);
+    d_sort = scratch + kStaticOrderBytes;
+  }
   cudaError_t e = run_eval(tree, params, d_queries, nq, d_results, d_contribs, d_ord, d_sort,
                            static_cast<cudaStream_t>(stream_ptr));
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");

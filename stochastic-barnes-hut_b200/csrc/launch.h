@@ -10,10 +10,12 @@ namespace sbh {
 cudaError_t launch_brute_force(const DevTree& t, int kernel, const float* q, long long nq,
                                const KParams& kp, float* out, cudaStream_t stream, int sm_count);
 
+// stage_leaves: accepted multi-point leaves are copied to shared memory by bulk
+// asynchronous copies (SBH_FLAG_STAGE_LEAVES; not with vote).
 cudaError_t launch_barnes_hut(const DevTree& t, int kernel, bool vote, const float* q,
                               long long nq, const int* order, float beta, const KParams& kp,
                               float* out, int* contribs, int* status, cudaStream_t stream,
-                              int sm_count);
+                              int sm_count, bool stage_leaves = false);
 
 // self_mass (optional, indexed like the queries): subtract each query's own
 // source term, as batched requests may ask.  query_base: index of q[0] within

@@ -12,33 +12,43 @@
 //     continuation probabilities; average the samples.
 //   result = sum of BH terms + sum of averaged corrections.
 //
-// B200 mapping: one warp per query; lanes never walk a node's children one by
-// one while the others wait.
-//   * Expansions.  Whenever some lanes each need the children sum of a node
-//     (its "expansion"), the warp lays the children of all those nodes out as
-//     one flat list and evaluates it 32 entries at a time -- consecutive
-//     children are consecutive node records, so the loads coalesce -- and a
-//     segmented scan across the lanes (one segment per node) forms every
-//     node's children sum at once, so no lane adds children one by one while
-//     the others wait.
-//   * Phase A, lanes over subdomains: the BH term of S and the first path step
-//     from S (taken by every sample of S: its continuation probability is 1),
-//     expanded once per subdomain instead of once per sample.
-//   * Phase B, lanes over sampled paths (32 at a time), advanced in lock step:
-//     every lane decides its Russian roulette step and finds the next node, then
-//     the warp expands all nodes the step needs together.  Each path draws its
-//     own Philox4x32-10 stream keyed by (seed, query index, path index), so
-//     results do not depend on launch shape, batching or query order.
-//   * The per-path corrections and BH terms are added in the reference's order:
-//     each subdomain's paths left to right by the first lane holding one of
-//     them, the subdomains' means and the BH terms by lane 0.
+// B200 mapping: a warp takes 32 queries at a time (sbh_warp_task, tasks.cuh).
+//   * First level, lane per query.  Every sample of S takes its first step with
+//     probability 1 and weight |S| / (1 x |S|) = 1, adding
+//     sum_{children c of S} k(c) - k(S); with S's BH term k(S) that is sum_c k(c)
+//     whatever the sample.  So the first-level part of the estimate is the sum
+//     of k over the root's grandchildren (plus the points of leaf subdomains):
+//     one contiguous range of node records (children are numbered breadth
+//     first), summed like a brute force -- the warp stages 32 records at a time
+//     in shared memory and every lane reads them back as broadcasts for its own
+//     query.  The reference evaluates that expansion once per sample.
+//   * Deeper steps, one query at a time, lane per path.  A bulk step takes each
+//     path's sample point, its first step to the node c1 below S that holds the
+//     point (its path code gives the cell at every level) and the Russian
+//     roulette at c1; the few paths that continue go into a shared-memory queue.
+//     Whenever 32 are queued (and once at the end), the warp advances them in
+//     lock step: every lane decides its Russian roulette step and finds the
+//     next node, then the warp expands all nodes the step needs together -- the
+//     children of all those nodes as one flat list, 32 entries at a time
+//     (consecutive children are consecutive records, so the loads coalesce),
+//     and a segmented scan across the lanes forms every node's children sum.
+//     So rounds start full, instead of 32 paths of which most stop after one
+//     step waiting on the longest.
+//   * Each path draws its own Philox4x32-10 stream keyed by (seed, query index,
+//     path index) -- word 0 the sample point, then one word per Russian
+//     roulette decision, as the reference draws them -- so results do not
+//     depend on launch shape, batching or query order.
+//   * The deeper steps of a query's surviving paths are added in path order and
+//     divided by samples_per_subdomain once; the estimate is the first-level
+//     sum plus that.
 // With identical random decisions the estimator takes exactly the reference
-// CPU estimator's paths and terms, each term rounded as the reference rounds it
-// (IEEE single rounding, see device_common.cuh); only each node's children sum
-// is added as a balanced tree instead of left to right.  The oracle drives its
-// restatement with the same Philox stream: contribution counts match exactly
-// and values to a few ulp of the summed magnitudes.  The reference's GPU
-// kernel (seed 0, streams shared across queries, per-block sample indices,
+// CPU estimator's paths and terms (each term rounded as the reference rounds
+// it, see device_common.cuh), grouped differently: the reference adds k(S),
+// then per sample the first-step difference and the deeper steps, and divides
+// each subdomain's sum by the sample count.  The oracle drives its restatement
+// with the same Philox stream: contribution counts match exactly and values to
+// a few ulp of the summed magnitudes.  The reference's GPU kernel (seed 0,
+// streams shared across queries, per-block sample indices,
 // tree_sampler_gpu.h:41-42,69-71) is replaced by independent per-query streams.
 #include "launch.h"
 #include "tasks.cuh"
@@ -60,22 +70,14 @@ __global__ void __launch_bounds__(SBH_THREADS, 8)
                       KParams kp, float* __restrict__ out, int* __restrict__ contribs,
                       int* status, const float* __restrict__ self_mass, long long query_base) {
   extern __shared__ float s_mem[];
-  const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const SbhWarpSmem<float> ws = sbh_carve<float>(
-      s_mem + (size_t)warp * sbh_warp_words<float>(t.root_children), t.root_children);
+  const SbhWarpSmem<float> ws = sbh_carve<float>(s_mem + (size_t)warp * sbh_warp_words<float>());
+  const long long units = (nq + 31) / 32;
   const long long stride = (long long)gridDim.x * SBH_WARPS;
-  for (long long slot = (long long)blockIdx.x * SBH_WARPS + warp; slot < nq; slot += stride) {
-    const long long qi = order ? (long long)__ldg(order + slot) : slot;
-    float r;
-    int c;
-    const float3 q = load_query<DIM>(qsoa, nq, qi);
-    sbh_query<DIM, K>(t, q, PART ? query_base + qi : qi, samples, seed, kp, ws, status, r, c);
-    if (lane == 0) {
-      if (PART && self_mass) r = rsub(r, self_term<DIM, K>(q, __ldg(self_mass + qi), kp));
-      out[qi] = r;
-      if (contribs) contribs[qi] = c;
-    }
+  for (long long u = (long long)blockIdx.x * SBH_WARPS + warp; u < units; u += stride) {
+    sbh_warp_task<DIM, K>(t, qsoa, nq, order, u * 32, min(nq, u * 32 + 32),
+                          PART ? query_base : 0, samples, seed, kp, ws, status, out, contribs,
+                          PART ? self_mass : nullptr);
   }
 }
 
@@ -84,14 +86,17 @@ cudaError_t launch_sbh_variant(const DevTree& t, const float* q, long long nq, c
                        int samples, unsigned long long seed, const KParams& kp, float* out,
                        int* contribs, int* status, cudaStream_t stream, int sm_count,
                        const float* self_mass, long long query_base) {
-  const size_t smem = (size_t)SBH_WARPS * sbh_warp_words<float>(t.root_children) * sizeof(float);
+  const size_t smem = (size_t)SBH_WARPS * sbh_warp_words<float>() * sizeof(float);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(stochastic_kernel<DIM, K, PART>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  long long blocks = (nq + SBH_WARPS - 1) / SBH_WARPS;
-  const long long cap = (long long)sm_count * 64;
+  // A warp takes 32 queries at a time; blocks beyond the resident ones are
+  // handed out as earlier ones finish, which balances uneven query costs.
+  const long long units = (nq + 31) / 32;
+  long long blocks = (units + SBH_WARPS - 1) / SBH_WARPS;
+  const long long cap = (long long)sm_count * 256;
   if (blocks > cap) blocks = cap;
   stochastic_kernel<DIM, K, PART><<<(unsigned)blocks, SBH_THREADS, smem, stream>>>(
       t, q, nq, order, samples, seed, kp, out, contribs, status, self_mass, query_base);

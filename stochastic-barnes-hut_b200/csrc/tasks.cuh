@@ -16,6 +16,15 @@ struct BhStackEntry {
   unsigned mask;  // lanes that visit this sibling range
 };
 
+// A warp's shared-memory buffer for the points of an accepted leaf, filled by
+// bulk asynchronous copies (bh_warp_task with STAGE).
+struct BhLeafStage {
+  float4 pm[32];   // position, mass
+  float4 nrm[32];  // normal (winding number only)
+  uint64_t bar;    // completion barrier of the copies
+  uint64_t pad;
+};
+
 // Kernel value of a query's own source (mass m at the query point): the term a
 // caller excludes when the queries are the sources themselves.
 template <int DIM, int K, class A = SumF<DIM, K>>
@@ -39,7 +48,13 @@ __device__ __forceinline__ typename A::V self_term(float3 q, float m, const KPar
 // self_mass (optional, indexed like the queries) subtracts each query's own
 // source term.  The sums follow the policy A (sums.cuh); `grads` receives the
 // gradient when A carries one.
-template <int DIM, int K, bool VOTE, class A = SumF<DIM, K>>
+//
+// STAGE (single-call kernel, leaf sizes above 1): when some lanes accept a leaf
+// holding several points, lane 0 copies the leaf's point records into the
+// warp's BhLeafStage with bulk asynchronous copies (cp.async.bulk, 32 points at
+// a time) and the accepting lanes read them from shared memory; the same
+// values in the same order, so results are identical.
+template <int DIM, int K, bool VOTE, class A = SumF<DIM, K>, bool STAGE = false>
 __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __restrict__ qsoa,
                                              long long nq, const int* __restrict__ order,
                                              long long slot0, long long slot_end, float beta,
@@ -47,7 +62,8 @@ __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __re
                                              int* __restrict__ contribs, int* status,
                                              BhStackEntry* stk, int stack_cap,
                                              const float* __restrict__ self_mass,
-                                             float* __restrict__ grads = nullptr) {
+                                             float* __restrict__ grads = nullptr,
+                                             BhLeafStage* stage = nullptr) {
   const int lane = threadIdx.x & 31;
   const long long slot = slot0 + lane;
   const bool valid = slot < slot_end;
@@ -58,7 +74,11 @@ __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __re
 
   typename A::V total = A::zero();
   int nc = 0;
-  if (lane == 0) stk[0] = BhStackEntry{0, 1, active};
+  uint32_t phase = 0;  // STAGE: parity of the stage barrier's current phase
+  if (lane == 0) {
+    stk[0] = BhStackEntry{0, 1, active};
+    if (STAGE) mbar_init(&stage->bar, 1);
+  }
   __syncwarp();
   int sp = 1;
   long long budget = t.nn + 1;  // a walk visits each node at most once
@@ -91,7 +111,35 @@ __device__ __forceinline__ void bh_warp_task(const DevTree& t, const float* __re
       const unsigned rej = __ballot_sync(0xffffffffu, in && !acc);
       acc = in && rej == 0u;
     }
-    if (acc) {
+    if (STAGE && leaf && topo.w - topo.z > 1) {
+      // (leaf and topo are the same on every lane: one node per step)
+      if (__any_sync(0xffffffffu, acc)) {
+        for (int c = topo.z; c < topo.w; c += 32) {
+          const int m = min(32, topo.w - c);
+          __syncwarp();  // every lane is done reading the previous chunk
+          if (lane == 0) {
+            fence_proxy_async_smem();
+            const uint32_t bytes = (uint32_t)m * 16u;
+            mbar_arrive_expect(&stage->bar, K == kWindingNumber ? 2u * bytes : bytes);
+            bulk_copy_g2s(stage->pm, t.pt_pm + c, bytes, &stage->bar);
+            if (K == kWindingNumber) bulk_copy_g2s(stage->nrm, t.pt_nrm + c, bytes, &stage->bar);
+          }
+          if (!mbar_wait_bounded(&stage->bar, phase, 1 << 20)) {
+            if (lane == 0) report_status(status, kStatusCopyTimeout);
+            mbar_wait_bounded(&stage->bar, phase, 1 << 20);  // the copy is still ours
+          }
+          phase ^= 1u;
+          if (acc) {
+            for (int i = 0; i < m; i++) {
+              const float4 nr =
+                  K == kWindingNumber ? stage->nrm[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+              total = A::add(total, A::point(stage->pm[i], nr, q, kp));
+              nc++;
+            }
+          }
+        }
+      }
+    } else if (acc) {
       if (leaf && topo.w - topo.z != 1) {
         for (int i = topo.z; i < topo.w; i++) {
           total = A::add(total, A::point(__ldg(t.pt_pm + i), __ldg(t.pt_nrm + i), q, kp));
@@ -290,58 +338,54 @@ __device__ __forceinline__ int contained_in_child(const DevTree& t, int v, int4 
 }
 
 
-// Shared-memory scratch of one warp running the sampler (sbh_warp_words<V>
-// 4-byte words; V is the policy's value): the fixed-size arrays first, then
-// the three per-subdomain arrays, all found from the base and R so that the
-// warp keeps one pointer, not five.  Lane 0's running sums of the paths live
-// here too, not in registers every lane would carry through the paths.
+// Shared-memory scratch of one warp running the sampler: sbh_warp_words<V>()
+// 4-byte words (V is the policy's value), carved from one base pointer.
 template <class V>
 struct SbhWarpSmem {
   float* base;
-  int R;
   static constexpr int W = (int)(sizeof(V) / 4);
+  static constexpr int kQueue = 64;  // survivor queue capacity (31 waiting + 32 new)
+  static constexpr int kEntry = 8;   // words per queue entry
   // [32] lanes of the current expansion's owners, in order
   __device__ __forceinline__ int* ownlane() const { return reinterpret_cast<int*>(base); }
   // [4][32] the paths' pending random words (PathRng; word w of lane l at [w][l])
   __device__ __forceinline__ uint32_t* rngbuf() const {
     return reinterpret_cast<uint32_t*>(base + 32);
   }
-  // [32] each path's sampled point and [32] its subdomain's point count (as a
-  // float): read once per step, so they wait here rather than in registers
+  // [32] each lane's path: sampled point, its subdomain's point count (as a
+  // float) and the point's path code as two words (low [32], high [32])
   __device__ __forceinline__ int* path_point() const { return reinterpret_cast<int*>(base + 160); }
   __device__ __forceinline__ float* path_spi() const { return base + 192; }
-  // [32] each path's sampled point's path code, as two words (low [32], high [32])
   __device__ __forceinline__ uint32_t* path_code() const {
     return reinterpret_cast<uint32_t*>(base + 224);
   }
-  // [32] per-path corrections of the current round
-  __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 288); }
-  // lane 0's fold of the paths: [0] the control-variate sum, [1] the current
-  // subdomain's sum of path corrections; then the current subdomain's index
-  __device__ __forceinline__ V* fold() const { return reinterpret_cast<V*>(base + 288 + 32 * W); }
-  __device__ __forceinline__ int* fold_sub() const {
-    return reinterpret_cast<int*>(base + 288 + 34 * W);
-  }
-  // [R] BH term of each subdomain
-  __device__ __forceinline__ V* bhS() const {
-    return reinterpret_cast<V*>(base + 289 + 34 * W);
-  }
-  // [R] first-step difference of each subdomain
-  __device__ __forceinline__ V* diffS() const { return bhS() + R; }
-  // [R] contributions of that difference (-1: a leaf subdomain)
-  __device__ __forceinline__ int* ccS() const { return reinterpret_cast<int*>(diffS() + R); }
+  // [32][8] records staged for the first-level sum: (x, y, z, mass), (normal,
+  // flag); flag < 0 marks a leaf whose points are summed instead
+  __device__ __forceinline__ float4* tile() const { return reinterpret_cast<float4*>(base + 288); }
+  // [kQueue][kEntry] surviving paths: path index, sampled point, node to
+  // expand, next node, path probability, running ratio, next node's depth,
+  // pending random word
+  __device__ __forceinline__ int* queue() const { return reinterpret_cast<int*>(base + 544); }
+  // [32] per-query flags (bit 0: NaN result) and contribution counts of the
+  // deeper path steps
+  __device__ __forceinline__ int* qflag() const { return reinterpret_cast<int*>(base + 1056); }
+  __device__ __forceinline__ int* qcount() const { return reinterpret_cast<int*>(base + 1088); }
+  // [32] a round's per-path sums, [32] per-query sums of the deeper steps and
+  // [32] per-query first-level sums
+  __device__ __forceinline__ V* pathv() const { return reinterpret_cast<V*>(base + 1120); }
+  __device__ __forceinline__ V* qsum() const { return reinterpret_cast<V*>(base + 1120 + 32 * W); }
+  __device__ __forceinline__ V* qacc() const { return reinterpret_cast<V*>(base + 1120 + 64 * W); }
 };
 
 template <class V>
-__host__ __device__ constexpr int sbh_warp_words(int R) {
-  return (int)(sizeof(V) / 4) * (2 * R + 34) + R + 289;
+__host__ __device__ constexpr int sbh_warp_words() {
+  return 1120 + 96 * (int)(sizeof(V) / 4);
 }
 
 template <class V>
-__device__ __forceinline__ SbhWarpSmem<V> sbh_carve(float* base, int R) {
+__device__ __forceinline__ SbhWarpSmem<V> sbh_carve(float* base) {
   SbhWarpSmem<V> w;
   w.base = base;
-  w.R = R;
   return w;
 }
 
@@ -354,196 +398,344 @@ __device__ __forceinline__ float path_weight(const DevTree& t, int v, float spi,
   return rdiv(spi, rmul(ev, (float)(unsigned)(tv.w - tv.z)));
 }
 
-// The whole estimator for one query, one warp: see sampler.cu for the method.
-// qi is the query's index in its request (it keys the Philox streams).  The
-// result and its contribution count are returned on lane 0.  Sums follow the
-// policy A; the sampled paths depend only on the tree, the query and the
-// random streams, so every policy walks the same paths for the same seed.
-template <int DIM, int K, class A = SumF<DIM, K>>
-__device__ __forceinline__ void sbh_query(const DevTree& t, float3 q, long long qi, int samples,
-                                          unsigned long long seed, const KParams& kp,
-                                          const SbhWarpSmem<typename A::V>& ws, int* status,
-                                          typename A::V& result, int& count) {
-  using V = typename A::V;
+// acc += k over the records [b, e) for this lane's query: node records
+// (NODES) or point records, staged 32 at a time by the warp in shared memory
+// and read back as broadcasts, the next chunk prefetched into registers.  A
+// node record that is a leaf holding several points (or none) stands for its
+// points, added in order.  Returns the number of kernel evaluations (the same
+// on every lane).  All lanes must call.
+template <bool NODES, class A>
+__device__ __forceinline__ long long sum_records(const DevTree& t, long long b, long long e,
+                                                 float3 q, const KParams& kp, float4* tile,
+                                                 typename A::V& acc) {
   const int lane = threadIdx.x & 31;
-  const int R = t.root_children;
-  const float inf = __int_as_float(0x7f800000);
-  const int c0 = __ldg(t.nd_topo).x;
-  result = A::zero();
-  count = 0;
-  if (R == 0) return;  // a single-leaf tree has no subdomains (tree_sampler.h:214)
-  int cnt = 0;
-
-// Phase A: BH term and first-step difference of every subdomain.
-  for (int g = 0; g < R; g += 32) {
-    const int j = g + lane;
-    const bool have = j < R;
-    int4 tS = make_int4(0, 0, 0, 0);
-    if (have) {
-      tS = __ldg(t.nd_topo + c0 + j);
-      // a leaf subdomain's points are added in order by lane 0 below
-      cnt += tS.y != 0 ? 1 : tS.w - tS.z;
+  long long cnt = 0;
+  float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
+  auto fetch = [&](long long base) {
+    const long long i = base + lane;
+    if (i < e) {
+      if (NODES) {
+        const float4 cm = __ldg(t.nd_cm + i), ag = __ldg(t.nd_agg + i);
+        r0 = make_float4(cm.x, cm.y, cm.z, ag.x);
+        r1 = make_float4(ag.y, ag.z, ag.w, cm.w);
+      } else {
+        r0 = __ldg(t.pt_pm + i);
+        const float4 nr = __ldg(t.pt_nrm + i);
+        r1 = make_float4(nr.x, nr.y, nr.z, 0.f);
+      }
     }
-    const bool own = have && tS.y != 0;
-    V kS = A::zero();
-    if (own) kS = A::node(__ldg(t.nd_cm + c0 + j), __ldg(t.nd_agg + c0 + j), q, kp);
-    int cc;
-    const V sumc = expand<A>(t, own, c0 + j, tS, q, kp, lane, ws.ownlane(), cc);
-    if (have) {
-      ws.bhS()[j] = kS;
-      ws.diffS()[j] = own ? A::sub(sumc, kS) : A::zero();
-      ws.ccS()[j] = own ? cc : -1;  // -1: a leaf subdomain (no path leaves it)
+  };
+  fetch(b);
+  for (long long base = b; base < e; base += 32) {
+    const int n = (int)min(32LL, e - base);
+    __syncwarp();
+    tile[2 * lane] = r0;
+    tile[2 * lane + 1] = r1;
+    __syncwarp();
+    fetch(base + 32);
+    for (int r = 0; r < n; r++) {
+      const float4 pm = tile[2 * r], nr = tile[2 * r + 1];
+      if (NODES && nr.w < 0.f) {  // a leaf holding several points (or none): its points
+        const int4 tc = __ldg(t.nd_topo + base + r);
+        for (int i = tc.z; i < tc.w; i++)
+          acc = A::add(acc, A::point(__ldg(t.pt_pm + i), __ldg(t.pt_nrm + i), q, kp));
+        cnt += tc.w - tc.z;
+      } else {
+        acc = A::add(acc, A::point(pm, make_float4(nr.x, nr.y, nr.z, 0.f), q, kp));
+        cnt++;
+      }
     }
   }
   __syncwarp();
+  return cnt;
+}
 
-  // Phase B: sampled paths, 32 at a time, advanced step by step in lock step.
-  const int P = R * samples;
-  if (lane == 0) {
-    ws.fold()[0] = A::zero();  // sum over subdomains of their mean path correction
-    ws.fold()[1] = A::zero();  // the current subdomain's sum of path corrections
-    *ws.fold_sub() = -1;
+// One lock-step round over n (<= 32) surviving paths of one query, taken
+// from the front of the queue: lane l continues path l.  A survivor has taken
+// its first step (out of its subdomain S) and passed its Russian roulette at
+// the next node c1; what is left is c1's step (the children sum of c1 minus
+// k(c1), weighted) and the steps after it, exactly as in the reference loop
+// (include/tree_sampler.h:66-110).  Every lane decides its Russian roulette
+// step and finds its next node, then the warp expands all nodes the step needs
+// together (expand()).  Each path's sum of its steps is left in pathv[l]; the
+// contribution count of the round is returned on every lane.
+template <int DIM, int K, class A>
+__device__ __forceinline__ int sbh_round(const DevTree& t, float3 q, long long key, int samples,
+                                         unsigned long long seed, const KParams& kp,
+                                         const SbhWarpSmem<typename A::V>& ws, int n, int* status,
+                                         bool& poisoned) {
+  using V = typename A::V;
+  const int lane = threadIdx.x & 31;
+  const int c0 = __ldg(t.nd_topo).x;
+  const int* e = ws.queue() + lane * SbhWarpSmem<V>::kEntry;
+  bool own = lane < n, active = false;
+  int pid = 0, prev = 0, cur = 0, dcur = 0;
+  float ev = 1.f, cb = 1.f;
+  int4 tprev = make_int4(0, 0, 0, 0), tcur = tprev;
+  PathRng rng;
+  rng.n = 3;
+  if (own) {
+    pid = e[0];
+    const int idx = e[1];
+    prev = e[2];
+    cur = e[3];
+    ev = __int_as_float(e[4]);
+    cb = __int_as_float(e[5]);
+    dcur = e[6];
+    ws.rngbuf()[96 + lane] = (uint32_t)e[7];
+    const unsigned long long code = __ldg(t.pt_code + idx);
+    ws.path_code()[lane] = (uint32_t)code;
+    ws.path_code()[32 + lane] = (uint32_t)(code >> 32);
+    ws.path_point()[lane] = idx;
+    const int4 tS = __ldg(t.nd_topo + c0 + pid / samples);
+    ws.path_spi()[lane] = (float)(unsigned)(tS.w - tS.z);
+    const int4 tp4 = __ldg(t.nd_topo + prev);
+    tprev = make_int4(tp4.x, tp4.y, 0, 0);
+    const int4 tc4 = __ldg(t.nd_topo + cur);
+    tcur = make_int4(tc4.x, tc4.y, 0, 0);
+    active = tcur.y != 0;
   }
-  for (int pbase = 0; pbase < P; pbase += 32) {
-    const int pid = pbase + lane;
-    V wd = A::zero();
-    bool active = false, first = false;  // first: the next step leaves the subdomain's root
-    int cur = 0;
-    int4 tcur = make_int4(0, 0, 0, 0);  // first child and child count of cur
-    float ev = 1.f, cb = 1.f;
-    int dcur = 1;                    // depth of cur
-    PathRng rng;
-    if (pid < P) {
-      const int S = c0 + pid / samples;
-      const int4 tS = __ldg(t.nd_topo + S);
-      rng.begin();
-      const uint32_t nS = (uint32_t)(tS.w - tS.z);
-      const int idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)qi, (uint32_t)pid,
-                                            ws.rngbuf() + lane);
-      const unsigned long long code = __ldg(t.pt_code + idx);
-      ws.path_code()[lane] = (uint32_t)code;
-      ws.path_code()[32 + lane] = (uint32_t)(code >> 32);
-      ws.path_point()[lane] = idx;
-      ws.path_spi()[lane] = (float)nS;
-      cur = S;
-      tcur = make_int4(tS.x, tS.y, 0, 0);
-      const float r0 = tS.y == 0 ? inf : far_field_ratio<DIM>(__ldg(t.nd_cm + S), q);
-      cb = (1.f < r0) ? r0 : 1.f;
-      active = tS.y != 0;
-      first = true;
+  V term = A::zero();
+  int cnt = 0;
+  while (__any_sync(0xffffffffu, own)) {
+    int cc;
+    const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, ws.ownlane(), cc);
+    if (own) {
+      const float w = path_weight(t, prev, ws.path_spi()[lane], ev);
+      const V kprev = A::node(__ldg(t.nd_cm + prev), __ldg(t.nd_agg + prev), q, kp);
+      term = A::add(term, A::scale(w, A::sub(sumc, kprev)));
+      cnt += cc;
     }
-    while (__any_sync(0xffffffffu, active)) {
-      bool own = false;
-      int prev = 0;
-      int4 tprev = make_int4(0, 0, 0, 0);
-      if (active) {
-        const float4 cmc = __ldg(t.nd_cm + cur);
-        const float ffr = far_field_ratio<DIM>(cmc, q);
-        const float ratio = rdiv(cb, ffr);
-        const float tp = (1.f < ratio) ? 1.f : ratio;
-        const float u =
-            rng.uniform(seed, (unsigned long long)qi, (uint32_t)pid, ws.rngbuf() + lane);
-        if (u > tp) {
+    own = false;
+    if (active) {
+      const float ffr = far_field_ratio<DIM>(__ldg(t.nd_cm + cur), q);
+      const float ratio = rdiv(cb, ffr);
+      const float tp = (1.f < ratio) ? 1.f : ratio;
+      const float u = rng.uniform(seed, (unsigned long long)key, (uint32_t)pid, ws.rngbuf() + lane);
+      if (u > tp) {
+        active = false;
+      } else {
+        ev = rmul(ev, tp);
+        prev = cur;
+        tprev = tcur;
+        int4 tnext;
+        cur = contained_in_child<DIM>(t, prev, tprev, dcur, ws.path_code() + lane,
+                                      ws.path_point() + lane, tnext, dcur);
+        if (cur < 0) {
+          report_status(status, kStatusNullChild);
+          poisoned = true;
           active = false;
         } else {
-          ev = rmul(ev, tp);
-          prev = cur;
-          tprev = tcur;
-          int4 tnext;
-          cur = contained_in_child<DIM>(t, prev, tprev, dcur, ws.path_code() + lane,
-                                        ws.path_point() + lane, tnext, dcur);
-          if (cur < 0) {
-            report_status(status, kStatusNullChild);
-            wd = A::nan();
-            active = false;
-          } else {
-            cb = (cb < ffr) ? ffr : cb;
-            if (first) {
-              const float w = path_weight(t, prev, ws.path_spi()[lane], ev);
-              const int j = pid / samples;
-              wd = A::add(wd, A::scale(w, ws.diffS()[j]));
-              cnt += ws.ccS()[j];
-              first = false;
-            } else {
-              own = true;
-            }
-            tcur = make_int4(tnext.x, tnext.y, 0, 0);
-            if (tcur.y == 0) active = false;
-          }
+          cb = (cb < ffr) ? ffr : cb;
+          own = true;
+          tcur = make_int4(tnext.x, tnext.y, 0, 0);
+          if (tcur.y == 0) active = false;
         }
-      }
-      int cc;
-      const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, ws.ownlane(), cc);
-      if (own) {
-        // The step's weight is formed here, after the expansion, so that it is
-        // not carried through it.
-        const float w = path_weight(t, prev, ws.path_spi()[lane], ev);
-        const V kprev = A::node(__ldg(t.nd_cm + prev), __ldg(t.nd_agg + prev), q, kp);
-        wd = A::add(wd, A::scale(w, A::sub(sumc, kprev)));
-        cnt += cc;
       }
     }
-    ws.pathv()[lane] = wd;
-    // Fold the round's paths into the estimate, in path order: each run of
-    // consecutive paths of one subdomain (a group) is summed left to right by
-    // its first lane -- the first group continuing the previous round's last
-    // one from its carried partial sum -- and the completed groups' means are
-    // added to the running sum in group order by lane 0.  The same additions
-    // in the same order as one lane walking every path.
-    const V carry = ws.fold()[1];
-    const int carry_sub = *ws.fold_sub();
-    __syncwarp();
-    {
-      const unsigned full = 0xffffffffu;
-      const int m = min(32, P - pbase);  // paths in this round
-      const int jl = lane < m ? (pbase + lane) / samples : -1;
-      const int jprev = __shfl_up_sync(full, jl, 1);
-      const bool head = lane < m && (lane == 0 || jprev != jl);
-      const unsigned heads = __ballot_sync(full, head);
-      bool complete = false;
-      if (head) {
-        const unsigned later = lane == 31 ? 0u : heads & ~((2u << lane) - 1u);
-        const int end = later ? __ffs(later) - 1 : m;
-        V sum = (lane == 0 && jl == carry_sub) ? carry : A::zero();
-        for (int k = lane; k < end; k++) sum = A::add(sum, ws.pathv()[k]);
-        complete = end < m || pbase + m == P || (pbase + m) / samples != jl;
-        if (complete) ws.pathv()[lane] = A::div(sum, (float)samples);  // its own slot, read
-        if (later == 0) {                                                // the round's last group
-          if (complete) {
-            *ws.fold_sub() = -1;
-          } else {
-            ws.fold()[1] = sum;
-            *ws.fold_sub() = jl;
+  }
+  ws.pathv()[lane] = term;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  return cnt;
+}
+
+// The stochastic estimator (multiLevelPrefixControlVariateSample_stackless,
+// include/tree_sampler.h:21-113) for the queries at sorted positions
+// [slot0, slot_end) (at most 32), one warp: see sampler.cu for the method.
+// The random streams of query qi are keyed by key_base + qi (its index within
+// its request).  Results go to out/grads (policy A) and contribs, with each
+// query's own source term subtracted when self_mass is given.
+template <int DIM, int K, class A = SumF<DIM, K>>
+__device__ __forceinline__ void sbh_warp_task(
+    const DevTree& t, const float* __restrict__ qsoa, long long nq, const int* __restrict__ order,
+    long long slot0, long long slot_end, long long key_base, int samples,
+    unsigned long long seed, const KParams& kp, const SbhWarpSmem<typename A::V>& ws,
+    int* status, float* __restrict__ out, int* __restrict__ contribs,
+    const float* __restrict__ self_mass, float* __restrict__ grads = nullptr) {
+  using V = typename A::V;
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int nqw = (int)min(32LL, slot_end - slot0);
+  if (nqw <= 0) return;
+  const int R = t.root_children;
+  const int c0 = __ldg(t.nd_topo).x;
+  // The lane's own query (lane < nqw), reloaded where needed rather than
+  // carried through the path loop.
+  auto query_index = [&](int l) -> long long {
+    return order ? (long long)__ldg(order + slot0 + l) : slot0 + l;
+  };
+
+  // ---- First level, lane per query.  Every path's first step leaves its
+  // subdomain S with probability 1 and weight |S| / (1 x |S|) = 1 and adds
+  // sum_{children c of S} k(c) - k(S); together with S's Barnes-Hut term k(S)
+  // that is sum_c k(c), the same for every sample of S.  So the first-level
+  // part of the estimate is the sum of k over the root's grandchildren, plus
+  // the points of root children that are leaves -- the records of one
+  // contiguous range (children are numbered breadth first), summed here like
+  // a brute force over them.
+  V acc = A::zero();
+  long long cntA = 0;
+  {
+  const float3 q = lane < nqw ? load_query<DIM>(qsoa, nq, query_index(lane))
+                              : make_float3(0.f, 0.f, 0.f);
+  int l2b = 0x7fffffff, l2e = -1, nint = 0;
+  long long l2n = 0;
+  for (int g = 0; g < R; g += 32) {
+    const int j = g + lane;
+    const int4 tS = j < R ? __ldg(t.nd_topo + c0 + j) : make_int4(0, 0, 0, 0);
+    const bool internal = j < R && tS.y != 0;
+    nint += __popc(__ballot_sync(full, internal));
+    l2b = min(l2b, internal ? tS.x : 0x7fffffff);
+    l2e = max(l2e, internal ? tS.x + tS.y : -1);
+    l2n += internal ? tS.y : 0;
+    // Leaf subdomains: their points (the Barnes-Hut term of a leaf; no path leaves it).
+    for (unsigned m = __ballot_sync(full, j < R && !internal); m != 0u; m &= m - 1u) {
+      const int b = __ffs(m) - 1;
+      const int z = __shfl_sync(full, tS.z, b), w = __shfl_sync(full, tS.w, b);
+      cntA += sum_records<false, A>(t, z, w, q, kp, ws.tile(), acc);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    l2b = min(l2b, __shfl_xor_sync(full, l2b, o));
+    l2e = max(l2e, __shfl_xor_sync(full, l2e, o));
+    l2n += __shfl_xor_sync(full, l2n, o);
+  }
+  bool layout_ok = true;
+  if (nint > 0) {
+    layout_ok = l2n == (long long)l2e - l2b;
+    if (layout_ok) cntA += (long long)samples * sum_records<true, A>(t, l2b, l2e, q, kp,
+                                                                        ws.tile(), acc);
+    cntA += nint;  // each internal subdomain's Barnes-Hut term
+  }
+  if (!layout_ok && lane == 0) report_status(status, kStatusNullChild);
+  ws.qflag()[lane] = layout_ok ? 0 : 1;
+  ws.qcount()[lane] = (int)cntA;
+  ws.qacc()[lane] = acc;
+  }
+  __syncwarp();
+
+  // ---- Deeper steps, one query at a time, lanes over its R x samples paths.
+  const int P = R * samples;
+  for (int k = 0; k < nqw; k++) {
+    const long long qik = query_index(k);
+    const float3 qk = load_query<DIM>(qsoa, nq, qik);
+    const long long key = key_base + qik;
+    bool poisoned = false;
+    int queued = 0, cntB = 0;
+    if (lane == 0) ws.qsum()[k] = A::zero();  // the surviving paths' deeper steps, in path order
+    for (int pbase = 0; pbase < P; pbase += 32) {
+      // Bulk step, lane per path: sample the point, take the first step (out
+      // of S, always taken) and the Russian roulette at the node c1 it leads
+      // to.  Only paths that continue past c1 are queued.
+      const int pid = pbase + lane;
+      bool surv = false;
+      int idx = 0, c1 = 0, c2 = 0, d2 = 0;
+      float ev = 1.f, cb = 1.f;
+      PathRng rng;
+      if (pid < P) {
+        const int S = c0 + pid / samples;
+        const int4 tS = __ldg(t.nd_topo + S);
+        if (tS.y != 0) {
+          rng.begin();
+          const uint32_t nS = (uint32_t)(tS.w - tS.z);
+          idx = tS.z + (int)rng.index(nS, seed, (unsigned long long)key, (uint32_t)pid,
+                                     ws.rngbuf() + lane);
+          const unsigned long long code = __ldg(t.pt_code + idx);
+          ws.path_code()[lane] = (uint32_t)code;
+          ws.path_code()[32 + lane] = (uint32_t)(code >> 32);
+          ws.path_point()[lane] = idx;
+          // Russian roulette at S: traverse probability min(max(1, r) / r, 1),
+          // which is 1 unless r is NaN (then the reference's weight is NaN).
+          const float r0 = far_field_ratio<DIM>(__ldg(t.nd_cm + S), qk);
+          cb = (1.f < r0) ? r0 : 1.f;
+          const float ratio0 = rdiv(cb, r0);
+          const float tp0 = (1.f < ratio0) ? 1.f : ratio0;
+          rng.uniform(seed, (unsigned long long)key, (uint32_t)pid, ws.rngbuf() + lane);
+          if (!(tp0 == 1.f)) poisoned = true;
+          int4 tc1;
+          int d1;
+          c1 = contained_in_child<DIM>(t, S, tS, 1, ws.path_code() + lane,
+                                       ws.path_point() + lane, tc1, d1);
+          if (c1 < 0) {
+            report_status(status, kStatusNullChild);
+            poisoned = true;
+          } else if (tc1.y != 0) {
+            const float r1 = far_field_ratio<DIM>(__ldg(t.nd_cm + c1), qk);
+            const float ratio1 = rdiv(cb, r1);
+            const float tp1 = (1.f < ratio1) ? 1.f : ratio1;
+            const float u1 =
+                rng.uniform(seed, (unsigned long long)key, (uint32_t)pid, ws.rngbuf() + lane);
+            if (!(u1 > tp1)) {
+              ev = rmul(rmul(1.f, tp0), tp1);
+              int4 tc2;
+              c2 = contained_in_child<DIM>(t, c1, tc1, d1, ws.path_code() + lane,
+                                           ws.path_point() + lane, tc2, d2);
+              if (c2 < 0) {
+                report_status(status, kStatusNullChild);
+                poisoned = true;
+              } else {
+                cb = (cb < r1) ? r1 : cb;
+                surv = true;
+              }
+            }
           }
         }
       }
-      const unsigned done = __ballot_sync(full, head && complete);
-      __syncwarp();
-      if (lane == 0) {
-        V mlcv = ws.fold()[0];
-        for (unsigned d = done; d != 0u; d &= d - 1u) mlcv = A::add(mlcv, ws.pathv()[__ffs(d) - 1]);
-        ws.fold()[0] = mlcv;
+      const unsigned sm = __ballot_sync(full, surv);
+      if (surv) {
+        int* e = ws.queue() + (queued + __popc(sm & ((1u << lane) - 1u))) * SbhWarpSmem<V>::kEntry;
+        e[0] = pid;
+        e[1] = idx;
+        e[2] = c1;
+        e[3] = c2;
+        e[4] = __float_as_int(ev);
+        e[5] = __float_as_int(cb);
+        e[6] = d2;
+        e[7] = (int)ws.rngbuf()[96 + lane];
       }
+      queued += __popc(sm);
+      __syncwarp();
+      // Full rounds while 32 or more paths wait; the rest wait for the next
+      // bulk step (or the final round).
+      const bool last = pbase + 32 >= P;
+      while (queued >= 32 || (last && queued > 0)) {
+        const int n = min(queued, 32);
+        cntB += sbh_round<DIM, K, A>(t, qk, key, samples, seed, kp, ws, n, status, poisoned);
+        __syncwarp();
+        if (lane == 0) {
+          V dsum = ws.qsum()[k];
+          for (int r = 0; r < n; r++) dsum = A::add(dsum, ws.pathv()[r]);
+          ws.qsum()[k] = dsum;
+        }
+        // move the waiting entries to the front
+        for (int w = lane; w < (queued - n) * SbhWarpSmem<V>::kEntry; w += 32)
+          ws.queue()[w] = ws.queue()[n * SbhWarpSmem<V>::kEntry + w];
+        queued -= n;
+        __syncwarp();
+      }
+    }
+    const bool any_poison = __any_sync(full, poisoned);
+    if (lane == 0) {
+      ws.qcount()[k] += cntB;
+      if (any_poison) ws.qflag()[k] |= 1;
     }
     __syncwarp();
   }
 
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-  if (lane == 0) {
-    const V mlcv = ws.fold()[0];  // every group completed in the last round
-    V bh = A::zero();
-    for (int j = 0; j < R; j++) {
-      if (ws.ccS()[j] < 0) {  // a leaf subdomain: its points, in order
-        bh = add_leaf_points<A>(t, __ldg(t.nd_topo + c0 + j), q, kp, bh);
-      } else {
-        bh = A::add(bh, ws.bhS()[j]);
-      }
+  if (lane < nqw) {
+    const long long qi = query_index(lane);
+    V r = R == 0 ? A::zero() : A::add(ws.qacc()[lane], A::div(ws.qsum()[lane], (float)samples));
+    if (ws.qflag()[lane] & 1) r = A::nan();
+    if (self_mass) {
+      const float3 q = load_query<DIM>(qsoa, nq, qi);
+      r = A::sub(r, self_term<DIM, K, A>(q, __ldg(self_mass + qi), kp));
     }
-    result = A::add(bh, mlcv);
-    count = cnt;
+    A::store(out, grads, nq, qi, r, kp);
+    if (contribs) contribs[qi] = ws.qcount()[lane];
   }
-  __syncwarp();  // the next query of this warp overwrites the scratch
+  __syncwarp();  // the warp's next queries overwrite the scratch
 }
 
 // ======================================================= brute force ===

@@ -31,6 +31,7 @@ ERR_UNSUPPORTED = 6
 GRAVITY, WINDING_NUMBER, SMOOTH_DIST, PLUMMER = 0, 1, 2, 3
 BRUTE_FORCE, BARNES_HUT, BARNES_HUT_VOTE, STOCHASTIC = 0, 1, 2, 3
 FLAG_KEEP_ORDER = 0x1
+FLAG_STAGE_LEAVES = 0x2
 
 # Every function the header declares, with its ctypes signature.
 _P = ctypes.c_void_p
