@@ -221,7 +221,8 @@ int sbh_eval_batch(const sbh_batch_item* items, int n_items, void* stream);
  * sampler's streams are keyed by query index, Barnes-Hut is exact per query);
  * only the speed does. */
 typedef struct sbh_batch_tuning {
-  int32_t sampler_unit_queries; /* sampler queries per work unit, 1..64 (default 2) */
+  int32_t sampler_unit_queries; /* sampler queries per work unit, 1..64 (default 32: the
+                                   first-level sum evaluates a unit's queries a lane each) */
   int32_t bucket_queries;       /* target queries per Morton bucket, 2..4096 (default 8) */
   int32_t blocks_per_sm;        /* persistent CTAs per SM; 0 = as many as fit (default) */
   int32_t bh_unit_queries;      /* Barnes-Hut queries per warp walk, 1..32 (default 32; the

@@ -68,7 +68,8 @@ class BatchEngine {
  public:
   // Schedule knobs (the autotuner's search space); results never depend on them.
   struct Tuning {
-    int sampler_unit = 2;     // sampler queries per work unit
+    int sampler_unit = 32;    // sampler queries per work unit (the first-level
+                              // sum runs a lane per query of a unit)
     int bucket_queries = 8;   // target queries per Morton bucket
     int blocks_per_sm = 0;    // persistent CTAs per SM (0: as many as fit)
     int bh_unit = 32;         // Barnes-Hut queries per warp walk (1..32)

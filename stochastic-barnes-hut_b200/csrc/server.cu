@@ -422,7 +422,7 @@ SBH_API int sbh_batch_autotune(const sbh_batch_item* items, int n_items, void* s
             std::find(values.begin(), values.end(), v) == values.end())
           values.push_back(v);
     } else if (coord == 1) {
-      values = {1, 2, 4, 8};
+      values = {32, 16, 8, 64};
     } else if (coord == 2) {
       values = {4, 8, 16, 32};
     } else if (coord == 3) {

@@ -91,7 +91,7 @@ def test_batch_tuning_defaults_and_range_checks():
     """sbh_batch_tuning_init's defaults, and sbh_batch_set_tuning's refusals,
     which happen on the host before any device is touched."""
     t = C.batch_tuning()
-    assert t.as_dict() == {"sampler_unit_queries": 2, "bucket_queries": 8, "blocks_per_sm": 0,
+    assert t.as_dict() == {"sampler_unit_queries": 32, "bucket_queries": 8, "blocks_per_sm": 0,
                            "bh_unit_queries": 32, "direct_queries": 65536}
     import pytest
     for bad in (dict(sampler_unit_queries=0), dict(bucket_queries=1), dict(blocks_per_sm=-1),
