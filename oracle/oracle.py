@@ -76,6 +76,7 @@ def oracle_lib() -> ctypes.CDLL:
         lib.orc_bh_grad.argtypes = [_P, ctypes.c_int, _P, _I64, _F, _F, _F, _P, _P, _P]
         lib.orc_sbh_grad.argtypes = [_P, ctypes.c_int, _P, _I64, ctypes.c_int, ctypes.c_uint64,
                                      _F, _F, _P, _P, _P]
+        lib.orc_bh_indexed.argtypes = lib.orc_bh.argtypes
         lib.orc_sbh_deepest.argtypes = [_P, ctypes.c_int, _P, _I64, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_uint64, _P, _F, _P]
         lib.orc_sbh_grad_rng.argtypes = [_P, ctypes.c_int, _P, _I64, ctypes.c_int, ctypes.c_int,
@@ -223,6 +224,18 @@ class OracleTree(_TreeBase):
         hs = np.zeros(nq, np.uint64)
         self.lib.orc_bh(self._h, kernel, _ptr(q), nq, float(np.float32(beta)), eps, _ptr(out),
                         _ptr(cnt), _ptr(hs))
+        return out, cnt, hs
+
+    def bh_indexed(self, kernel, queries, beta, eps=1e-3):
+        """bh() with sibling steps by index instead of nextChild's midpoint
+        quantization (see orc_bh_indexed)."""
+        q = _f32(queries, (-1, self.dim))
+        nq = q.shape[0]
+        out = np.zeros(nq, np.float32)
+        cnt = np.zeros(nq, np.int32)
+        hs = np.zeros(nq, np.uint64)
+        self.lib.orc_bh_indexed(self._h, kernel, _ptr(q), nq, float(np.float32(beta)), eps,
+                                _ptr(out), _ptr(cnt), _ptr(hs))
         return out, cnt, hs
 
     def bh_vote(self, kernel, queries, beta, eps=1e-3, group=32):

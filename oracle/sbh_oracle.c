@@ -588,9 +588,20 @@ static int64_t contained_in_child(const orc_tree* t, int64_t v, const float* p) 
   return -1;
 }
 
-/* evaluateBarnesHut_stackless, include/barnes_hut.h:23-78. */
-static float bh_one(const orc_tree* t, int kernel, const float* q, float beta, float eps,
-                    int32_t* ncontrib, uint64_t* hash) {
+/* The sibling after child c of p in cell order, by index: a node's children
+ * are numbered consecutively in cell order (include/tree3d.h:291-301), so it is
+ * c + 1 while that is still a child of p.  This is what nextChild computes
+ * when quantizing the child's midpoint lands in the child's own cell. */
+static int64_t next_child_indexed(const orc_tree* t, int64_t p, int64_t c) {
+  const int64_t fc = first_child(t, p);
+  return (fc >= 0 && c + 1 < fc + t->nch[p]) ? c + 1 : -1;
+}
+
+/* evaluateBarnesHut_stackless, include/barnes_hut.h:23-78.  With `indexed`
+ * the sibling steps use next_child_indexed instead of nextChild's midpoint
+ * quantization (the same walk wherever the quantization is exact). */
+static float bh_walk(const orc_tree* t, int kernel, const float* q, float beta, float eps,
+                     int32_t* ncontrib, uint64_t* hash, int indexed) {
   enum { FROM_CHILD, FROM_PARENT, FROM_SIBLING };
   float total = 0;
   int nc = 0;
@@ -627,7 +638,7 @@ static float bh_one(const orc_tree* t, int kernel, const float* q, float beta, f
       return total;
     }
     int64_t p = t->parent[node];
-    int64_t nx = next_child(t, p, node);
+    int64_t nx = indexed ? next_child_indexed(t, p, node) : next_child(t, p, node);
     if (nx < 0) {
       node = p;
       state = FROM_CHILD;
@@ -638,6 +649,11 @@ static float bh_one(const orc_tree* t, int kernel, const float* q, float beta, f
   }
   if (ncontrib) *ncontrib = -1; /* traversal did not terminate */
   return NAN;
+}
+
+static float bh_one(const orc_tree* t, int kernel, const float* q, float beta, float eps,
+                    int32_t* ncontrib, uint64_t* hash) {
+  return bh_walk(t, kernel, q, beta, eps, ncontrib, hash, 0);
 }
 
 typedef struct {
@@ -662,6 +678,21 @@ static void bh_body(void* vc, int64_t i) {
   c->out[i] = bh_one(c->t, c->kernel, c->q + i * c->t->dim, c->beta, c->eps, &n, &h);
   if (c->counts) c->counts[i] = n;
   if (c->hashes) c->hashes[i] = h;
+}
+
+static void bh_indexed_body(void* vc, int64_t i) {
+  eval_ctx* c = (eval_ctx*)vc;
+  int32_t n = 0;
+  uint64_t h = 0;
+  c->out[i] = bh_walk(c->t, c->kernel, c->q + i * c->t->dim, c->beta, c->eps, &n, &h, 1);
+  if (c->counts) c->counts[i] = n;
+  if (c->hashes) c->hashes[i] = h;
+}
+
+void orc_bh_indexed(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta,
+                    float eps, float* out, int32_t* counts, uint64_t* hashes) {
+  eval_ctx c = {t, kernel, 0, 0, 0, q, nq, beta, eps, 0, NULL, out, counts, hashes, NULL, NULL};
+  par_for(nq, 16, bh_indexed_body, &c);
 }
 
 void orc_bh(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta, float eps,

@@ -96,6 +96,14 @@ void orc_sbh_grad(const orc_tree* t, int kernel, const float* q, int64_t nq, int
 void orc_sbh_deepest(const orc_tree* t, int kernel, const float* q, int64_t nq, int samples,
                      int rng_mode, uint64_t seed, const uint32_t* mt_seeds, float eps,
                      int32_t* deepest);
+/* orc_bh with the sibling steps taken by index (a node's children are
+ * consecutive in cell order) instead of nextChild's re-quantization of the
+ * child's midpoint (include/tree3d.h:193-206).  The two walks agree wherever
+ * that quantization is exact; at cell sizes near FP32 resolution nextChild can
+ * return a wrong sibling and the reference's walk skips children or never ends
+ * (orc_bh then reports count -1). */
+void orc_bh_indexed(const orc_tree* t, int kernel, const float* q, int64_t nq, float beta,
+                    float eps, float* out, int32_t* counts, uint64_t* hashes);
 /* orc_sbh_grad with the random stream of choice: ORC_RNG_PHILOX (seed, as
  * orc_sbh_grad) or ORC_RNG_MT19937 (the reference CPU sampler's std::mt19937
  * stream, seeded per query from mt_seeds, as orc_sbh). */

@@ -23,13 +23,14 @@ contribution counts, bit-identical values.
 Variance: the north star asks for per-query variance within 10% of the
 reference's at an equal budget.  The reference is the oracle's mt19937 sampler
 (the reference CPU's own std::mt19937 / uniform_real_distribution stream,
-pinned bit for bit by the golden vectors); the GPU draws Philox.  With 16,384
-replicates the noise of a variance ratio is about 2% per query (its standard
+pinned bit for bit by the golden vectors); the GPU draws Philox.  With 32,768
+replicates the noise of a variance ratio is about 1.5-2% per query (its standard
 error is estimated from the sample kurtosis of both replicate sets); every
 query whose ratio has a standard error of at most 3.3% must be within 10%
 outright, the others within 10% plus three standard errors, and at least 80%
 of the queries must be in the first group (60% for the heavy-tailed gradient
-of the smooth sum, with four times the replicates).
+of the smooth sum, with twice the replicates; the gravity gradient uses
+16,384).
 """
 import numpy as np
 import pytest
@@ -137,16 +138,27 @@ def test_sampler_paths_past_the_path_codes(dsl, samples, kernel):
                                      samples_per_subdomain=samples, seed=5), contribs=True)
     assert np.array_equal(cnt, rc)
     assert sampler_close(v, rv, sc)
-    # Barnes-Hut on the same deep tree, bit for bit.
-    bv, bc, _ = ot.bh(kernel, q, 2.0)
+    # Barnes-Hut on the same deep tree, bit for bit against the reference's walk
+    # with sibling steps by index.  The reference's own stackless walk finds the
+    # next sibling by re-quantizing the child's midpoint (nextChild,
+    # include/tree3d.h:193-206); at these cell sizes (near FP32 resolution) that
+    # can return a wrong sibling, and for one query of this tree the walk never
+    # ends (the compiled reference does not return; the oracle bounds it and
+    # reports -1).  Everywhere it ends it equals the indexed walk.
+    bv, bc, _ = ot.bh_indexed(kernel, q, 2.0)
+    sv, sc2, _ = ot.bh(kernel, q, 2.0)
+    ends = sc2 >= 0
+    assert ends.mean() > 0.99
+    assert np.array_equal(sc2[ends], bc[ends]) and bits_equal(sv[ends], bv[ends])
     g, _, gc = gpu.eval(q, C.params(method=C.BARNES_HUT, kernel=kernel, beta=2.0), contribs=True)
     assert np.array_equal(gc, bc)
     assert bits_equal(g, bv)
+    gpu.check()
 
 
 # ------------------------------------------------- per-query variance
 
-REPS = 16384
+REPS = 32768
 STRICT_SE = 0.033
 
 
@@ -221,7 +233,7 @@ def test_sampler_gradient_variance_per_query_matches_reference(kernel):
     # The smooth sum's gradient is heavy-tailed (rare paths close to the query
     # carry large weights): four times the replicates, and at least 60% of the
     # queries in the strict group.
-    reps, min_strict = (REPS, 0.8) if kernel == C.GRAVITY else (4 * REPS, 0.6)
+    reps, min_strict = (REPS // 2, 0.8) if kernel == C.GRAVITY else (2 * REPS, 0.6)
     q = W.uniform_queries(16, seed=57, dim=3, lo=-0.9, hi=0.9)
     qq = np.tile(q, (reps, 1))
     v, g, _ = gpu.eval_grad(qq, C.params(method=C.STOCHASTIC, kernel=kernel,

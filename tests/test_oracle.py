@@ -148,3 +148,20 @@ def test_gpu_fp64_brute_force_library_loads():
     and exports its entry point; running it needs a GPU."""
     lib = O.gpu_lib()
     assert hasattr(lib, "orc_gpu_brute_force_f64")
+
+
+def test_indexed_barnes_hut_walk_equals_the_stackless_walk(golden):
+    """orc_bh_indexed (sibling steps by index) is the reference's stackless walk
+    (nextChild by midpoint quantization) bit for bit -- values, counts and
+    accepted-node hashes -- on every golden tree, where the quantization is
+    exact."""
+    for name, g in golden.items():
+        ot = O.OracleTree(g["points"], g["normals"], g["masses"], g["min_corner"],
+                          g["max_corner"], alpha=float(g["alpha"]),
+                          dim_split_log=int(g["dim_split_log"]), leaf_size=int(g["leaf_size"]))
+        for kernel in (O.GRAVITY, O.WINDING_NUMBER, O.PLUMMER):
+            for beta in (2.0, 1.25):
+                a, ac, ah = ot.bh(kernel, g["queries"], beta)
+                b, bc, bh = ot.bh_indexed(kernel, g["queries"], beta)
+                assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), name
+                assert np.array_equal(ac, bc) and np.array_equal(ah, bh), name
