@@ -5,11 +5,12 @@ Default workload (the configuration the headline metric is quoted on): serving.
 surfaces; 10^4..2*10^6 points) and 1,500 seeded requests (a tree, a kernel --
 gravity, winding number or smooth distance with alpha 100 --, 1..10^5 queries in
 the tree's box, a sample budget 64/256/1024).  Both paths run at matched
-accuracy, median relative error <= 1e-3 against FP64 brute force per kernel:
-the plain per-call Barnes-Hut drop-in at each kernel's matched theta, the
-served path at each kernel's matched operating point (stochastic BH with the
-drawn budgets scaled per kernel, or Barnes-Hut where the stochastic estimate
-cannot reach the target); the errors are re-measured in every run.
+accuracy, median relative error <= 1e-3 against FP64 brute force per kernel
+(MATCHED): the plain per-call drop-in at Barnes-Hut's largest sufficient theta
+(exact summation where no theta suffices), the served path at the fastest
+operating point that meets the target; stochastic BH's own matched figures
+(where it meets the target) are reported beside.  The errors are re-measured in
+every run.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload serving|sbh_wn|bh_wn|plain_small_bf|plain_small_bh|
@@ -740,18 +741,25 @@ SERVING_KID = {"gravity": 0, "wn": 1, "smooth": 2}  # SBH_KERNEL_* (the referenc
 SERVING_ALPHA = 100.0
 MATCH_TARGET = 1e-3
 
-# Operating points at matched accuracy (median relative error <= 1e-3 against
-# FP64 brute force, per kernel, on the serving mix): the plain per-call
-# Barnes-Hut's opening angle theta, and for the served path the method and the
-# factor on every request's drawn sample budget (64/256/1024).  Chosen by
-# `python bench.py --workload serving --calibrate` (the largest theta and the
-# smallest budget factor that reach the target; a kernel whose stochastic
-# estimate does not reach it within 16x the budgets is served by Barnes-Hut at
-# its matched theta); every bench run re-measures the errors at these points.
+# Operating points at matched accuracy: median relative error <= 1e-3 against
+# FP64 brute force, per kernel, on the serving mix.  An operating point is
+# (method, parameter): ("barnes_hut", theta), ("stochastic", factor on every
+# request's drawn sample budget 64/256/1024) or ("brute_force", None).
+#   plain       the per-call drop-in: Barnes-Hut at the largest theta that meets
+#               the target, or exact summation where no theta of the ladder does
+#   stochastic  the smallest budget factor at which stochastic BH meets the
+#               target (None: not within 16x the drawn budgets)
+#   served      the fastest of the points that meet the target, by the batched
+#               throughput the calibration measures
+# Chosen by `python bench.py --workload serving --calibrate` (FP64 references of
+# 50 requests per kernel; the ladders and timings are kept with the profiles);
+# every bench run re-measures the errors at these points.
 MATCHED = {
-    "gravity": {"theta": 0.5, "served": "stochastic", "budget_scale": 1.0},
-    "wn": {"theta": 0.3, "served": "stochastic", "budget_scale": 4.0},
-    "smooth": {"theta": 0.1, "served": "barnes_hut", "budget_scale": None},
+    "gravity": {"plain": ("barnes_hut", 0.5), "stochastic": 0.25,
+                "served": ("barnes_hut", 0.5)},
+    "wn": {"plain": ("barnes_hut", 0.2), "stochastic": None, "served": ("barnes_hut", 0.2)},
+    "smooth": {"plain": ("brute_force", None), "stochastic": None,
+               "served": ("brute_force", None)},
 }
 CAL_THETAS = (0.8, 0.6, 0.5, 0.4, 0.3, 0.25, 0.2, 0.15, 0.1, 0.07, 0.05)
 CAL_SCALES = (0.25, 0.5, 1.0, 2.0, 4.0, 8.0, 16.0)
@@ -763,7 +771,8 @@ def serving_setup(C, seed=77, n_trees=32, n_requests=1500, device_trees=True):
     tree, kernel (gravity / winding number / smooth distance alpha 100), query
     count log-uniform in [1, 10^5] uniform in the tree's box, budget 64/256/1024.
     With device_trees the trees are built on the GPU in both layouts (Octree1 /
-    Quadtree1 for Barnes-Hut, Octree2 / Quadtree2 for the sampler)."""
+    Quadtree1 for Barnes-Hut and brute force, Octree2 / Quadtree2 for the
+    sampler)."""
     import sbh_workloads as W
     rng = np.random.default_rng(seed)
     trees = []
@@ -799,28 +808,32 @@ def serving_setup(C, seed=77, n_trees=32, n_requests=1500, device_trees=True):
     return trees, reqs
 
 
-def request_params(C, W, t, r, method, theta=None, budget_scale=None):
-    """Parameters of request r served by `method` ("stochastic" / "barnes_hut")
-    at the given operating point (default: the matched one of its kernel)."""
-    op = MATCHED[r["kernel"]]
+def request_params(C, W, t, r, op):
+    """Parameters of request r at operating point op = (method, parameter)."""
+    method, x = op
     kid = SERVING_KID[r["kernel"]]
     alpha = SERVING_ALPHA if r["kernel"] == "smooth" else None
     if method == "stochastic":
-        scale = op["budget_scale"] if budget_scale is None else budget_scale
-        scale = 1.0 if scale is None else scale
         return C.params(method=C.STOCHASTIC, kernel=kid, alpha=alpha, seed=r["nq"],
                         samples_per_subdomain=W.samples_for_budget(
-                            int(round(r["budget"] * scale)), t["root2"]))
-    th = op["theta"] if theta is None else theta
-    return C.params(method=C.BARNES_HUT, kernel=kid, alpha=alpha, beta=1.0 / th)
+                            int(round(r["budget"] * x)), t["root2"]))
+    if method == "barnes_hut":
+        return C.params(method=C.BARNES_HUT, kernel=kid, alpha=alpha, beta=1.0 / x)
+    return C.params(method=C.BRUTE_FORCE, kernel=kid, alpha=alpha)
 
 
-def served_method(r):
-    return MATCHED[r["kernel"]]["served"]
+def op_of(r, role):
+    """The operating point of request r in a role: "plain", "served", or
+    "served_stochastic" (stochastic BH where it meets the target, else the
+    served point)."""
+    m = MATCHED[r["kernel"]]
+    if role == "served_stochastic":
+        return ("stochastic", m["stochastic"]) if m["stochastic"] is not None else m["served"]
+    return m[role]
 
 
-def tree_for(t, method):
-    return t["sbh"] if method == "stochastic" else t["bh"]
+def tree_key(op):
+    return "sbh" if op[0] == "stochastic" else "bh"
 
 
 def wait_until(t0, at):
@@ -832,26 +845,26 @@ def wait_until(t0, at):
 
 
 def drive_plain(C, W, trees, reqs, arrivals):
-    """The reference's usage: one blocking per-call Barnes-Hut evaluation per
-    request (host buffers, copies inside the call), in arrival order, at the
-    kernel's matched theta."""
+    """The reference's usage: one blocking per-call evaluation per request (host
+    buffers, copies inside the call), in arrival order, at each kernel's plain
+    operating point."""
     outs = []
     lat = []
     t0 = time.perf_counter()
     for r, at in zip(reqs, arrivals):
         wait_until(t0, at)
         t = trees[r["tree"]]
+        op = op_of(r, "plain")
         out = np.empty(r["nq"], np.float32)
-        t["bh"].eval_host_ptr(r["q"].ctypes.data, r["nq"], out.ctypes.data,
-                              request_params(C, W, t, r, "barnes_hut"))
+        t[tree_key(op)].eval_host_ptr(r["q"].ctypes.data, r["nq"], out.ctypes.data,
+                                      request_params(C, W, t, r, op))
         lat.append((time.perf_counter() - t0 - at) * 1e3)
         outs.append(out)
     return time.perf_counter() - t0, np.array(lat), outs
 
 
-def drive_served(C, W, trees, reqs, server, ids, arrivals, method=None):
-    """Requests submitted to the server at their arrival times (host buffers);
-    method None: each kernel's matched served method."""
+def drive_served(C, W, trees, reqs, server, ids, arrivals, role="served"):
+    """Requests submitted to the server at their arrival times (host buffers)."""
     handles = [None] * len(reqs)
     lateness = np.zeros(len(reqs))
 
@@ -860,9 +873,9 @@ def drive_served(C, W, trees, reqs, server, ids, arrivals, method=None):
             wait_until(t0, at)
             lateness[k] = (time.perf_counter() - t0 - at) * 1e3
             t = trees[r["tree"]]
-            mth = method or served_method(r)
-            handles[k] = server.submit(ids[(r["tree"], mth)], r["q"],
-                                       request_params(C, W, t, r, mth))
+            op = op_of(r, role)
+            handles[k] = server.submit(ids[(r["tree"], tree_key(op))], r["q"],
+                                       request_params(C, W, t, r, op))
 
     t0 = time.perf_counter()
     th = threading.Thread(target=submitter)
@@ -912,54 +925,81 @@ def serving_references(trees, reqs, per_kernel=30, n_max=1024, seed=5):
     return refs
 
 
-def median_errors(C, W, trees, reqs, refs, method, kernel, **op):
-    """Median error of `method` at an operating point over the picked requests
-    of one kernel (blocking calls on the first queries of each)."""
+def median_errors(C, W, trees, reqs, refs, kernel, op):
+    """(median, p99) error of an operating point over the picked requests of one
+    kernel (blocking calls on the first queries of each)."""
     errs = []
     for k, ref in refs.items():
         r = reqs[k]
         if r["kernel"] != kernel:
             continue
         t = trees[r["tree"]]
-        v, _ = tree_for(t, method).eval(r["q"][:len(ref)],
-                                        request_params(C, W, t, r, method, **op))
+        v, _ = t[tree_key(op)].eval(r["q"][:len(ref)], request_params(C, W, t, r, op))
         errs.append(serving_error(kernel, v, ref))
     e = np.concatenate(errs)
     return float(np.median(e)), float(np.percentile(e, 99))
 
 
-def serving_calibrate(C, W, trees, reqs, refs):
-    """The calibration ladders: median error per kernel for every plain theta
-    and every budget factor of the stochastic method."""
-    out = {}
-    for kern in SERVING_KERNELS:
-        rows = {"barnes_hut": {}, "stochastic": {}}
-        for th in CAL_THETAS:
-            rows["barnes_hut"][th] = median_errors(C, W, trees, reqs, refs, "barnes_hut", kern,
-                                                   theta=th)
-        for sc in CAL_SCALES:
-            rows["stochastic"][sc] = median_errors(C, W, trees, reqs, refs, "stochastic", kern,
-                                                   budget_scale=sc)
-        ok_th = [th for th in CAL_THETAS if rows["barnes_hut"][th][0] <= MATCH_TARGET]
-        ok_sc = [sc for sc in CAL_SCALES if rows["stochastic"][sc][0] <= MATCH_TARGET]
-        out[kern] = {"ladders": {m: {str(k): v for k, v in d.items()} for m, d in rows.items()},
-                     "theta": max(ok_th) if ok_th else None,
-                     "budget_scale": min(ok_sc) if ok_sc else None}
-    return out
-
-
-def device_batch(C, W, torch, trees, reqs, method_of):
-    """Batch entries for every request with its queries resident on the device."""
+def device_batch(C, W, torch, trees, reqs, role=None, op_for=None):
+    """Batch entries for every request with its queries resident on the device,
+    at its role's operating point (or op_for(r))."""
     entries, keep = [], []
     for r in reqs:
         t = trees[r["tree"]]
-        mth = method_of(r)
+        op = op_for(r) if op_for else op_of(r, role)
         dq = torch.from_numpy(np.ascontiguousarray(r["q"].T)).cuda()
         out = torch.empty(r["nq"], dtype=torch.float32, device="cuda")
-        entries.append((tree_for(t, mth), request_params(C, W, t, r, mth), dq.data_ptr(),
+        entries.append((t[tree_key(op)], request_params(C, W, t, r, op), dq.data_ptr(),
                         r["nq"], out.data_ptr(), 0, 0))
         keep += [dq, out]
     return entries, keep
+
+
+def batch_ms(C, torch, entries, repeats=3):
+    """Event-timed median of sbh_eval_batch over the entries (one untimed run first)."""
+    C.eval_batch(entries)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(repeats):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        C.eval_batch(entries)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def serving_calibrate(C, W, torch, trees, reqs, refs):
+    """The calibration ladders: per kernel, the median / p99 error and the
+    batched throughput (all requests of the kernel, queries resident) of every
+    Barnes-Hut theta, every stochastic budget factor and brute force; and the
+    operating points chosen from them."""
+    out = {}
+    for kern in SERVING_KERNELS:
+        sub = [r for r in reqs if r["kernel"] == kern]
+        nq = sum(r["nq"] for r in sub)
+        rows = []
+        ops = ([("barnes_hut", th) for th in CAL_THETAS] +
+               [("stochastic", sc) for sc in CAL_SCALES] + [("brute_force", None)])
+        for op in ops:
+            med, p99 = median_errors(C, W, trees, reqs, refs, kern, op)
+            entries, keep = device_batch(C, W, torch, trees, sub, op_for=lambda r: op)
+            ms = batch_ms(C, torch, entries, repeats=1 if op[0] == "brute_force" else 3)
+            del entries, keep
+            rows.append({"op": list(op), "median_rel_err": med, "p99_rel_err": p99,
+                         "batched_queries_per_s": nq / (ms / 1e3)})
+        meets = [x for x in rows if x["median_rel_err"] <= MATCH_TARGET]
+        bh = [x for x in meets if x["op"][0] == "barnes_hut"]
+        sb = [x for x in meets if x["op"][0] == "stochastic"]
+        out[kern] = {
+            "ladder": rows,
+            "plain": max(bh, key=lambda x: x["op"][1])["op"] if bh else ["brute_force", None],
+            "stochastic": min(x["op"][1] for x in sb) if sb else None,
+            "served": max(meets, key=lambda x: x["batched_queries_per_s"])["op"] if meets else None,
+        }
+    return out
 
 
 def run_serving(args):
@@ -969,40 +1009,42 @@ def run_serving(args):
     import sbh_workloads as W
     t_setup = time.perf_counter()
     trees, reqs = serving_setup(C)
-    refs = serving_references(trees, reqs)
     if args.calibrate:
-        return {"calibration": serving_calibrate(C, W, trees, reqs, refs),
-                "target": MATCH_TARGET, "requests_per_kernel": len(refs) // 3}
+        refs = serving_references(trees, reqs, per_kernel=50)
+        return {"calibration": serving_calibrate(C, W, torch, trees, reqs, refs),
+                "target": MATCH_TARGET, "requests_per_kernel": 50,
+                "reference": "FP64 brute force on the GPU, first 1,024 queries per request"}
+    refs = serving_references(trees, reqs)
     total_q = sum(r["nq"] for r in reqs)
 
-    # Accuracy at the matched operating points (and of the stochastic method on
-    # every kernel at its configured budgets, for reference).
+    # Accuracy at the matched operating points, and of stochastic BH at the
+    # requests' own budgets for comparison.
     acc = {}
     for kern in SERVING_KERNELS:
-        op = MATCHED[kern]
-        acc[kern] = {
-            "plain_barnes_hut": dict(zip(("median_rel_err", "p99_rel_err"), median_errors(
-                C, W, trees, reqs, refs, "barnes_hut", kern)), theta=op["theta"]),
-            "served": dict(zip(("median_rel_err", "p99_rel_err"), median_errors(
-                C, W, trees, reqs, refs, op["served"], kern)), method=op["served"],
-                budget_scale=op["budget_scale"]),
-            "stochastic_at_drawn_budgets": dict(zip(("median_rel_err", "p99_rel_err"),
-                                                    median_errors(C, W, trees, reqs, refs,
-                                                                  "stochastic", kern,
-                                                                  budget_scale=1.0))),
-        }
-    matched = all(max(a["plain_barnes_hut"]["median_rel_err"], a["served"]["median_rel_err"])
+        m = MATCHED[kern]
+        row = {}
+        for role in ("plain", "served", "served_stochastic"):
+            op = op_of({"kernel": kern}, role)
+            med, p99 = median_errors(C, W, trees, reqs, refs, kern, op)
+            row[role] = {"op": list(op), "median_rel_err": med, "p99_rel_err": p99}
+        med, p99 = median_errors(C, W, trees, reqs, refs, kern, ("stochastic", 1.0))
+        row["stochastic_at_drawn_budgets"] = {"median_rel_err": med, "p99_rel_err": p99}
+        row["stochastic_meets_target"] = m["stochastic"] is not None
+        acc[kern] = row
+    matched = all(max(a[r]["median_rel_err"] for r in ("plain", "served", "served_stochastic"))
                   <= MATCH_TARGET for a in acc.values())
 
     # Batch schedule for the served path, autotuned on the first 256 requests (untimed).
-    entries, keep = device_batch(C, W, torch, trees, reqs[:256], served_method)
+    entries, keep = device_batch(C, W, torch, trees, reqs[:256], "served")
     tuning, best_ms, start_ms = C.batch_autotune(entries, stream=0, repeats=2)
     torch.cuda.synchronize()
     del entries, keep
 
     # value: the whole request stream as one batched evaluation with every
-    # request's queries resident in HBM, at the matched operating points.
-    entries, keep = device_batch(C, W, torch, trees, reqs, served_method)
+    # request's queries resident in HBM, at the served operating points.
+    n_direct = sum(1 for r in reqs if op_of(r, "served")[0] == "stochastic" and
+                   tuning.direct_queries > 0 and r["nq"] >= tuning.direct_queries)
+    entries, keep = device_batch(C, W, torch, trees, reqs, "served")
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     with ClockSampler(0) as clocks:
@@ -1010,12 +1052,17 @@ def run_serving(args):
                               flush, args.warmup, args.steps)
     del entries, keep
     dev_total_ms = float(sum(dev_ms))
+    entries, keep = device_batch(C, W, torch, trees, reqs, "served_stochastic")
+    dev_sbh_ms = statistics.mean(timed_device(
+        lambda: C.eval_batch(entries, stream=stream.cuda_stream), stream, flush, 1,
+        max(2, args.steps // 4)))
+    del entries, keep
 
     server = C.Server(slots=3, slot_queries=1 << 20, max_requests_per_batch=4096, tuning=tuning)
     ids = {}
     for i, t in enumerate(trees):
-        ids[(i, "stochastic")] = server.add_tree(t["sbh"])
-        ids[(i, "barnes_hut")] = server.add_tree(t["bh"])
+        ids[(i, "sbh")] = server.add_tree(t["sbh"])
+        ids[(i, "bh")] = server.add_tree(t["bh"])
     setup_s = time.perf_counter() - t_setup
     # Warm-up of every path on a slice of the stream.
     warm = reqs[:50]
@@ -1028,8 +1075,8 @@ def run_serving(args):
     plain_rps = len(reqs) / plain_mk
     # Served capacity (e2e): the same stream submitted at t = 0, host buffers.
     served_mk, served_lat, _ = drive_served(C, W, trees, reqs, server, ids, np.zeros(len(reqs)))
-    served_bh_mk, _, _ = drive_served(C, W, trees, reqs, server, ids, np.zeros(len(reqs)),
-                                      method="barnes_hut")
+    sbh_mk, sbh_lat, _ = drive_served(C, W, trees, reqs, server, ids, np.zeros(len(reqs)),
+                                      role="served_stochastic")
     rates = {}
     rng = np.random.default_rng(5)
     for factor in (0.5, 1.0, 2.0):
@@ -1037,7 +1084,7 @@ def run_serving(args):
         gaps = rng.exponential(1.0 / rate, len(reqs))
         arrivals = np.cumsum(gaps) - gaps[0]
         row = {"arrival_rate_rps": rate}
-        for name, fn in (("plain_barnes_hut", lambda: drive_plain(C, W, trees, reqs, arrivals)),
+        for name, fn in (("plain", lambda: drive_plain(C, W, trees, reqs, arrivals)),
                          ("served", lambda: drive_served(C, W, trees, reqs, server, ids,
                                                          arrivals))):
             mk, lat, _ = fn()
@@ -1047,6 +1094,7 @@ def run_serving(args):
     stats = server.stats()
     server.close()
     served_qps = total_q / served_mk
+    plain_qps = total_q / plain_mk
     cpu = None
     if not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -1055,10 +1103,10 @@ def run_serving(args):
             cq, cs, cn, _ = reference_serving_sample(trees, reqs, args.cpu_seconds)
             cores = O.ref_hardware_concurrency()
             cpu = {"value": cq / cs, "unit": "queries/s", "cores": cores, "kind": "reference",
-                   "sample": f"the first {cn} requests of the stream ({int(cq)} queries), "
-                             f"src/sbh.cpp evalBarnesHut at each kernel's matched theta, its "
-                             f"thread pool ({cores} threads), {cs:.1f} s"}
-    plain_qps = total_q / plain_mk
+                   "sample": f"the first {cn} requests of the stream ({int(cq)} queries, at most "
+                             f"{REF_QUERIES_PER_REQUEST} per request), src/sbh.cpp evalBarnesHut "
+                             f"at each kernel's plain operating point (beta = inf for exact), "
+                             f"its thread pool ({cores} threads), {cs:.1f} s"}
     return {
         "metric": METRIC, "value": total_q / (dev_total_ms / args.steps / 1e3),
         "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -1074,12 +1122,18 @@ def run_serving(args):
                 "p50_ms": float(np.percentile(served_lat, 50)),
                 "p99_ms": float(np.percentile(served_lat, 99))},
         "served_over_plain": served_qps / plain_qps,
-        "plain_barnes_hut": {"queries_per_s": plain_qps, "requests_per_s": plain_rps,
-                             "p50_ms": float(np.percentile(plain_lat, 50)),
-                             "p99_ms": float(np.percentile(plain_lat, 99)),
-                             "path": "one blocking sbh_eval per request (host buffers), "
-                                     "Barnes-Hut at each kernel's matched theta"},
-        "served_barnes_hut_only": {"queries_per_s": total_q / served_bh_mk},
+        "plain": {"queries_per_s": plain_qps, "requests_per_s": plain_rps,
+                  "p50_ms": float(np.percentile(plain_lat, 50)),
+                  "p99_ms": float(np.percentile(plain_lat, 99)),
+                  "path": "one blocking sbh_eval per request (host buffers) at each kernel's "
+                          "plain operating point"},
+        "served_stochastic": {
+            "what": "the server with stochastic BH wherever it meets the target (gravity at the "
+                    "drawn budgets x MATCHED factor), the served points elsewhere",
+            "queries_per_s": total_q / sbh_mk, "over_plain": (total_q / sbh_mk) / plain_qps,
+            "p50_ms": float(np.percentile(sbh_lat, 50)),
+            "p99_ms": float(np.percentile(sbh_lat, 99)),
+            "device_batch_queries_per_s": total_q / (dev_sbh_ms / 1e3)},
         "matched": {"target_median_rel_err": MATCH_TARGET, "all_within_target": matched,
                     "operating_points": MATCHED, "accuracy": acc,
                     "reference": "FP64 brute force on the GPU (the oracle's libsbh_bf64.so), "
@@ -1089,7 +1143,10 @@ def run_serving(args):
         "autotune": {"tuning": tuning.as_dict(), "tuned_ms": best_ms, "default_ms": start_ms},
         "setup_s": setup_s,
         "cpu_baseline": cpu,
-        "gpu_launches": None,
+        # per batch step: the graph's 9 kernels (query boxes, keys, three scan
+        # kernels, scatter, one persistent kernel per method class) plus 8 (sort
+        # and sampler) per stochastic request sent to its own launch
+        "gpu_launches": args.steps * (9 + 8 * n_direct),
     }
 
 
@@ -1097,21 +1154,30 @@ def serving_config(n_requests, total_q):
     return {"workload": "serving: 32 resident trees (16 3D, 16 2D; Gaussian mixtures, torus, "
                         "sphere and circle surfaces; 1e4..2e6 points), 1500 seeded requests, "
                         "gravity / winding number / smooth distance (alpha 100), 1..1e5 "
-                        "queries log-uniform, budgets 64/256/1024 scaled per kernel to matched "
-                        "accuracy; served (continuous batching) vs plain per-call Barnes-Hut, "
-                        "both at median relative error <= 1e-3 vs FP64",
+                        "queries log-uniform, budgets 64/256/1024; served (continuous batching) "
+                        "vs plain per-call evaluation, both at each kernel's operating point of "
+                        "median relative error <= 1e-3 vs FP64",
+            "operating_points": {k: {"plain": list(v["plain"]), "served": list(v["served"]),
+                                     "stochastic_budget_factor": v["stochastic"]}
+                                 for k, v in MATCHED.items()},
             "requests": n_requests, "queries": total_q,
             "server": {"slots": 3, "slot_queries": 1 << 20},
             "l2": "512 MiB buffer written between timed batch steps"}
 
 
+REF_QUERIES_PER_REQUEST = 2048
+
+
 def reference_serving_sample(trees, reqs, budget_s, start=0, ref_trees=None):
     """The reference's CPU plugin (src/sbh.cpp evalBarnesHut, compiled unmodified
     in oracle/_ref, its own thread pool) on consecutive requests of the stream
-    from `start`, each at its kernel's matched theta, until `budget_s` seconds
-    of evaluation: (queries, seconds, requests, next start).  Reference trees
-    (Octree1 / Quadtree1, alpha 100) are built on first use; builds are not
-    timed."""
+    from `start`, each at its kernel's plain operating point (Barnes-Hut at the
+    matched theta, or beta = inf -- the reference's own exact evaluation,
+    python/example.py:76-82 -- where the plain point is exact), until
+    `budget_s` seconds of evaluation: (queries, seconds, requests, next start).
+    A request's first REF_QUERIES_PER_REQUEST queries stand for it (per-query
+    work is independent).  Reference trees (Octree1 / Quadtree1, alpha 100) are
+    built on first use; builds are not timed."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     ref_trees = {} if ref_trees is None else ref_trees
@@ -1124,10 +1190,11 @@ def reference_serving_sample(trees, reqs, budget_s, start=0, ref_trees=None):
         if r["tree"] not in ref_trees:
             ref_trees[r["tree"]] = O.RefTree(t["pts"], t["nrm"], t["m"], t["lo"], t["hi"],
                                              alpha=SERVING_ALPHA, dim_split_log=1)
-        _, s = ref_trees[r["tree"]].plugin_bh(SERVING_KID[r["kernel"]],
-                                              np.ascontiguousarray(r["q"]),
-                                              1.0 / MATCHED[r["kernel"]]["theta"])
-        nq += r["nq"]
+        method, theta = MATCHED[r["kernel"]]["plain"]
+        beta = 1.0 / theta if method == "barnes_hut" else np.inf
+        q = np.ascontiguousarray(r["q"][:REF_QUERIES_PER_REQUEST])
+        _, s = ref_trees[r["tree"]].plugin_bh(SERVING_KID[r["kernel"]], q, beta)
+        nq += len(q)
         secs += s
         done += 1
         k += 1
@@ -1156,8 +1223,9 @@ def run_reference_serving(args):
         nreq += n
     value = tq / ts
     cores = O.ref_hardware_concurrency()
-    sample = (f"{nreq} consecutive requests of the 1500-request stream ({int(tq)} queries), "
-              f"src/sbh.cpp evalBarnesHut per request at each kernel's matched theta, its thread "
+    sample = (f"{nreq} consecutive requests of the 1500-request stream ({int(tq)} queries, at "
+              f"most {REF_QUERIES_PER_REQUEST} per request), src/sbh.cpp evalBarnesHut per request "
+              f"at each kernel's plain operating point (beta = inf where it is exact), its thread "
               f"pool ({cores} threads); tree builds excluded")
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s",

@@ -200,10 +200,13 @@ __device__ __forceinline__ void run_sbh(const DevTree& t, const BatchItem& it, l
 }
 
 template <int DIM, int K>
-__device__ __forceinline__ void run_bf(const DevTree& t, const BatchItem& it, long long u) {
-  const long long s0 = u * kUnitQueriesWarp;
-  bf_warp_task<DIM, K>(t, it.q, it.nq, s0, min(it.nq, s0 + kUnitQueriesWarp), it.kp, it.out,
-                       it.contribs, it.self_mass);
+__device__ __forceinline__ void run_bf(const DevTree& t, const BatchItem& it, long long u,
+                                       float* scratch) {
+  const long long s0 = u * kBfUnitQueries;
+  SrcPair* src = reinterpret_cast<SrcPair*>(scratch);
+  NrmPair* nrm = reinterpret_cast<NrmPair*>(src + 32);
+  bf_warp_task<DIM, K>(t, it.q, it.nq, s0, min(it.nq, s0 + kBfUnitQueries), it.kp, it.out,
+                       it.contribs, it.self_mass, src, nrm);
 }
 
 template <int CLASS, int DIM, int K>
@@ -213,7 +216,7 @@ __device__ __forceinline__ void run_unit(const DevTree& t, const BatchItem& it, 
   const int* ord = it.sort_bits > 0 ? order + it.sort_base : nullptr;
   if (CLASS == kClassBh) run_bh<DIM, K>(t, it, u, ord, scratch, stack_cap, status);
   if (CLASS == kClassSbh) run_sbh<DIM, K>(t, it, u, ord, scratch, status);
-  if (CLASS == kClassBf) run_bf<DIM, K>(t, it, u);
+  if (CLASS == kClassBf) run_bf<DIM, K>(t, it, u, scratch);
 }
 
 template <int CLASS>
@@ -300,6 +303,7 @@ int class_warp_words(int cls, int bh_stack, int sbh_r) {
   int scratch = 0;
   if (cls == kClassBh) scratch = bh_stack * (int)sizeof(BhStackEntry) / 4;
   if (cls == kClassSbh) scratch = sbh_warp_words<float>();
+  if (cls == kClassBf) scratch = (int)(32 * (sizeof(SrcPair) + sizeof(NrmPair)) / 4);
   (void)sbh_r;
   return kTreeWords + kItemWords + (scratch + 3) / 4 * 4;
 }
@@ -431,9 +435,10 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
     it.unit_base = unit_base[batch_class(it.method)];
     // Work unit: sampler queries per warp (tuned); Barnes-Hut queries per warp
     // walk (tuned; vote keeps 32, its acceptance is defined over 32 queries);
-    // brute force 32 queries per warp.
+    // brute force 64 queries per warp (two per lane).
     it.unit_queries = it.method == 3   ? tuning.sampler_unit
                       : it.method == 1 ? tuning.bh_unit
+                      : it.method == 0 ? kBfUnitQueries
                                        : kUnitQueriesWarp;
     it.units = (it.nq + it.unit_queries - 1) / it.unit_queries;
     sort_base += it.nq;

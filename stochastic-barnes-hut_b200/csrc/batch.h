@@ -59,9 +59,9 @@ struct BatchHeader {
   unsigned long long next_unit[kClasses];  // work counters of the persistent kernels
 };
 
-// Queries per work unit (one warp task) of brute force: 32, a lane each.  The
-// sampler gives each query a warp and Barnes-Hut a lane; their unit sizes
-// (queries per warp task) are tuned.
+// Queries per work unit (one warp task) of warp-vote Barnes-Hut: 32, a lane
+// each (brute force takes kBfUnitQueries, two per lane).  The sampler's and
+// Barnes-Hut's unit sizes (queries per warp task) are tuned.
 constexpr int kUnitQueriesWarp = 32;
 
 class BatchEngine {

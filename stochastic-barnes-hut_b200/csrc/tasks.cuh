@@ -4,6 +4,7 @@
 #pragma once
 
 #include "device_common.cuh"
+#include "pairs.cuh"
 #include "sums.cuh"
 
 namespace sbh {
@@ -749,35 +750,72 @@ __device__ __forceinline__ void two_sum_add(float& hi, float& lo, float s) {
   lo += e;
 }
 
-// Brute force for one warp of queries (lane per query, sources read as warp
-// broadcasts): the batched path's brute-force task.  Plain FP32 sums over 64
-// sources, merged by two-sum, as brute_force.cu does.
+// Queries per work unit of the batched brute-force task: two per lane.
+constexpr int kBfUnitQueries = 64;
+
+// Brute force for up to 64 queries at positions [slot0, slot_end) of a request,
+// one warp: the batch's brute-force task.  Lane l holds queries slot0 + l and
+// slot0 + 32 + l as one packed pair (the single-call kernel's FP32x2
+// arithmetic, pairs.cuh); the warp stages 32 sources at a time in its shared
+// memory (src / nrm, 32 entries each) with every coordinate duplicated into
+// both halves of a float2, and every lane reads them back as broadcasts.  Plain
+// FP32 sums over each 32 sources, merged into a (sum, error) pair per query by
+// two-sum.
 template <int DIM, int K>
 __device__ __forceinline__ void bf_warp_task(const DevTree& t, const float* __restrict__ qsoa,
                                              long long nq, long long slot0, long long slot_end,
                                              const KParams& kp, float* __restrict__ out,
                                              int* __restrict__ contribs,
-                                             const float* __restrict__ self_mass) {
+                                             const float* __restrict__ self_mass, SrcPair* src,
+                                             NrmPair* nrm) {
+  constexpr bool kNormals = (K == kWindingNumber);
   const int lane = threadIdx.x & 31;
-  const long long qi = slot0 + lane;
-  const bool valid = qi < slot_end;
-  const float3 q = valid ? load_query<DIM>(qsoa, nq, qi) : make_float3(0.f, 0.f, 0.f);
-  float hi = 0.f, lo = 0.f;
-  for (long long b = 0; b < t.n; b += 64) {
-    const long long e = min(t.n, b + 64);
-    float part = 0.f;
-    for (long long i = b; i < e; i++) {
-      const float4 s = __ldg(t.pt_pm + i);
-      const float4 nr = K == kWindingNumber ? __ldg(t.pt_nrm + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-      part += kernel_fast<DIM, K>(s, nr, q, kp);
+  const long long qa = slot0 + lane, qb = slot0 + 32 + lane;
+  float3 a = make_float3(0.f, 0.f, 0.f), b = a;
+  if (qa < slot_end) a = load_query<DIM>(qsoa, nq, qa);
+  if (qb < slot_end) b = load_query<DIM>(qsoa, nq, qb);
+  const float2 nqx = make_float2(-a.x, -b.x), nqy = make_float2(-a.y, -b.y),
+               nqz = make_float2(-a.z, -b.z);
+  float hia = 0.f, loa = 0.f, hib = 0.f, lob = 0.f;
+  const NrmPair no_normal = {};
+  for (long long base = 0; base < t.n; base += 32) {
+    const int len = (int)min(32LL, t.n - base);
+    __syncwarp();  // every lane is done with the previous sources
+    if (lane < len) {
+      const float4 v = __ldg(t.pt_pm + base + lane);
+      src[lane] = SrcPair{dup(v.x), dup(v.y), dup(v.z), dup(v.w)};
+      if (kNormals) {
+        const float4 n = __ldg(t.pt_nrm + base + lane);
+        nrm[lane] = NrmPair{dup(n.x), dup(n.y), dup(n.z), dup(0.f)};
+      }
     }
-    two_sum_add(hi, lo, part);
+    __syncwarp();
+    float2 part = make_float2(0.f, 0.f);
+    if (len == 32) {
+#pragma unroll 8
+      for (int k = 0; k < 32; k++)
+        part = accumulate2<DIM, K>(part, src[k], kNormals ? nrm[k] : no_normal, nqx, nqy, nqz, kp);
+    } else {
+      for (int k = 0; k < len; k++)
+        part = accumulate2<DIM, K>(part, src[k], kNormals ? nrm[k] : no_normal, nqx, nqy, nqz, kp);
+    }
+    two_sum_add(hia, loa, part.x);
+    two_sum_add(hib, lob, part.y);
   }
-  if (valid) {
-    float v = hi + lo;
-    if (self_mass) v -= self_term<DIM, K>(q, __ldg(self_mass + qi), kp);
-    out[qi] = v;
-    if (contribs) contribs[qi] = (int)t.n;
+  float va = hia + loa, vb = hib + lob;
+  if (K == kGravity) {  // accumulate2 adds +m / (r + 0.1)
+    va = -va;
+    vb = -vb;
+  }
+  if (qa < slot_end) {
+    if (self_mass) va -= self_term<DIM, K>(a, __ldg(self_mass + qa), kp);
+    out[qa] = va;
+    if (contribs) contribs[qa] = (int)t.n;
+  }
+  if (qb < slot_end) {
+    if (self_mass) vb -= self_term<DIM, K>(b, __ldg(self_mass + qb), kp);
+    out[qb] = vb;
+    if (contribs) contribs[qb] = (int)t.n;
   }
 }
 

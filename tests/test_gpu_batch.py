@@ -48,6 +48,9 @@ REQUESTS = [
     ("circle2", C.STOCHASTIC, C.SMOOTH_DIST, 700, dict(samples_per_subdomain=1, seed=1)),
     ("circle2", C.BARNES_HUT_VOTE, C.GRAVITY, 300, dict(beta=2.0)),
     ("gauss1", C.BRUTE_FORCE, C.GRAVITY, 100, dict()),
+    ("torus2", C.BRUTE_FORCE, C.WINDING_NUMBER, 130, dict()),
+    ("circle2", C.BRUTE_FORCE, C.SMOOTH_DIST, 65, dict()),
+    ("gauss1", C.BRUTE_FORCE, C.PLUMMER, 1, dict()),
     ("torus2", C.STOCHASTIC, C.GRAVITY, 2000, dict(samples_per_subdomain=1, seed=2,
                                                    flags=C.FLAG_KEEP_ORDER)),
     ("gauss1", C.BARNES_HUT, C.PLUMMER, 0, dict(beta=2.0)),
