@@ -58,7 +58,11 @@ REQUESTS = [
 
 
 def _check_same(method, kernel, got, want):
-    if method == C.BRUTE_FORCE:
+    if method == C.BRUTE_FORCE and kernel == C.WINDING_NUMBER:
+        # sign-changing sums that cancel to ~1e-3 of their O(1) terms: compared
+        # in the winding number's natural unit (the jump across the surface)
+        assert np.allclose(got, want, rtol=2e-6, atol=2e-6)
+    elif method == C.BRUTE_FORCE:
         assert np.allclose(got, want, rtol=2e-6, atol=0)
     elif kernel == C.SMOOTH_DIST:
         assert np.allclose(got, want, rtol=1e-5, atol=1e-30)
