@@ -92,7 +92,7 @@ struct BatchContext {
   bool pending = false;
   // Side streams of the direct launches (forked from and joined back into the
   // caller's stream): two, so that one launch's last wave overlaps the next.
-  static constexpr int kSide = 2;
+  static constexpr int kSide = 4;
   cudaStream_t side[kSide] = {};
   cudaEvent_t fork = nullptr;
   cudaEvent_t join[kSide] = {};
