@@ -67,7 +67,7 @@ L2_FLUSH_BYTES = 512 << 20
 # figures are listed with the kernel's profile.  Null in the bench line when
 # the query count or budget is overridden.
 DRAM_TRAFFIC = {
-    "sbh_wn": None,
+    "sbh_wn": 5.4615e9 + 0.2162e9,
     "bh_wn": 307.58e6 + 31.53e6,
     "plain_small_bf": 1.85e6,
     "plain_small_bh": 3.36e6,
