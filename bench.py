@@ -1052,6 +1052,7 @@ def run_serving(args):
                               flush, args.warmup, args.steps)
     del entries, keep
     dev_total_ms = float(sum(dev_ms))
+    breakdown, roofline = serving_breakdown(C, W, torch, trees, reqs, stream, flush)
     entries, keep = device_batch(C, W, torch, trees, reqs, "served_stochastic")
     dev_sbh_ms = statistics.mean(timed_device(
         lambda: C.eval_batch(entries, stream=stream.cuda_stream), stream, flush, 1,
@@ -1139,6 +1140,7 @@ def run_serving(args):
                     "reference": "FP64 brute force on the GPU (the oracle's libsbh_bf64.so), "
                                  "first 1,024 queries of 30 seeded requests per kernel"},
         "latency_at_rates": rates,
+        "breakdown": breakdown, "roofline": roofline,
         "server_stats": stats, "clocks": clocks.summary(),
         "autotune": {"tuning": tuning.as_dict(), "tuned_ms": best_ms, "default_ms": start_ms},
         "setup_s": setup_s,
@@ -1148,6 +1150,44 @@ def run_serving(args):
         # and sampler) per stochastic request sent to its own launch
         "gpu_launches": args.steps * (9 + 8 * n_direct),
     }
+
+
+def serving_breakdown(C, W, torch, trees, reqs, stream, flush):
+    """Each kernel's requests batched alone at their served operating points
+    (device-resident, CUDA events): where the served batch's time goes, and the
+    roofline of the largest part.  A part whose served point is brute force is
+    bound by the MUFU pipe (a reciprocal square root and an exponential or
+    reciprocal per pair): its pairs per second against the measured MUFU rate
+    halved; a traversal part is issue-bound and reported in queries/s."""
+    parts = {}
+    for kern in SERVING_KERNELS:
+        sub = [r for r in reqs if r["kernel"] == kern]
+        entries, keep = device_batch(C, W, torch, trees, sub, "served")
+        ms = statistics.mean(timed_device(lambda: C.eval_batch(entries, stream=stream.cuda_stream),
+                                          stream, flush, 2, 3))
+        del entries, keep
+        op = MATCHED[kern]["served"]
+        parts[kern] = {"op": list(op), "ms": ms, "queries": sum(r["nq"] for r in sub),
+                       "pairs": sum(r["nq"] * trees[r["tree"]]["n"] for r in sub)}
+    top = max(parts, key=lambda k: parts[k]["ms"])
+    p = parts[top]
+    if p["op"][0] == "brute_force":
+        rates = C.measure_pipe_rates(0)
+        peak = rates["rsqrt_per_s"] / 2.0
+        achieved = p["pairs"] / (p["ms"] / 1e3)
+        roof = {"bound": "sfu", "kernel": "batch_eval_kernel (brute-force class), " + top,
+                "achieved": achieved, "peak": peak, "unit": "pairs/s", "frac": achieved / peak,
+                "peak_source": "measured MUFU rsqrt rate (sbh_measure_pipe_rates) / 2 MUFU "
+                               f"ops per pair: {rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
+                               f"{rates['sm_clock_mhz']:.0f} MHz",
+                "kernel_ms": p["ms"], "pairs_per_launch": p["pairs"], "traffic": None,
+                "note": f"the {top} requests batched alone; share of the summed parts "
+                        f"{p['ms'] / sum(x['ms'] for x in parts.values()):.2f}"}
+    else:
+        roof = {"bound": "issue", "kernel": "batch_eval_kernel, " + top,
+                "achieved": p["queries"] / (p["ms"] / 1e3), "peak": None, "unit": "queries/s",
+                "frac": None, "kernel_ms": p["ms"], "traffic": None}
+    return parts, roof
 
 
 def serving_config(n_requests, total_q):
