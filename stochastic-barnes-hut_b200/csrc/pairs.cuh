@@ -33,6 +33,13 @@ __device__ __forceinline__ float mufu_rcp(float x) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+// 2^x with one MUFU operation; subnormal results are kept (no .ftz), so a sum
+// of far terms does not flush to zero before the library exponential would.
+__device__ __forceinline__ float mufu_ex2(float x) {
+  float y;
+  asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float2 rsqrt2(float2 x) {
   return make_float2(mufu_rsqrt(x.x), mufu_rsqrt(x.y));
 }
@@ -79,9 +86,9 @@ __device__ __forceinline__ float2 accumulate2(float2 part, const SrcPair& s, con
       den = __fmul2_rn(dup(kFourPi), __ffma2_rn(r2, norm_from_sq(r2), dup(1e-5f)));
     }
     return __ffma2_rn(num, rcp2(den), part);
-  } else {  // smooth distance
-    const float2 t = __fmul2_rn(dup(-kp.alpha), norm_from_sq(r2));
-    return __fadd2_rn(part, make_float2(expf(t.x), expf(t.y)));
+  } else {  // smooth distance: exp(-alpha r) = 2^(-alpha log2(e) r)
+    const float2 t = __fmul2_rn(dup(-kp.alpha * 1.44269504088896341f), norm_from_sq(r2));
+    return __fadd2_rn(part, make_float2(mufu_ex2(t.x), mufu_ex2(t.y)));
   }
 }
 
