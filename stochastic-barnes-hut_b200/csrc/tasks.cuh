@@ -220,48 +220,29 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
   // Entry e of owner o is child (tv.x + e - excl) of o.
   const int node_off = tv.x - excl;
   const unsigned upto = lane == 31 ? full : (2u << lane) - 1u;  // chunk positions 0..lane
-  // The chunk starting at `base`: the node record lane r evaluates (-1 past the
-  // end) and its segment head.  Owner of entry e: the owner whose segment
-  // covers the chunk's first entry, advanced by the segments that start
-  // between there and e; every owner has at least one child, so segments are
-  // never empty.  The head is the last segment start at or before this lane
-  // (0: the segment runs on from the previous chunk).
-  auto chunk = [&](int base, int& head) -> int {
+  V acc = A::zero();
+  contribs = 0;
+  for (int base = 0; base < total; base += 32) {
+    const int e = base + lane;
+    // Owner of entry e: the owner whose segment covers the chunk's first entry,
+    // advanced by the segments that start between there and e.  Every owner
+    // has at least one child, so segments are never empty.
     const unsigned starts =
         __reduce_or_sync(full, (own && excl >= base && excl < base + 32) ? 1u << (excl - base) : 0u);
     const int first = __popc(__ballot_sync(full, own && excl <= base)) - 1;
     const int o = ownlane[min(first + __popc(starts & upto & ~1u), 31)];
     const int o_off = __shfl_sync(full, node_off, o);
-    head = max(31 - __clz(starts & upto), 0);
-    return base + lane < total ? o_off + base + lane : -1;
-  };
-  V acc = A::zero();
-  contribs = 0;
-  // Software pipeline: the next chunk's records are requested before the
-  // current chunk is evaluated and scanned, so their load latency overlaps
-  // that work.
-  int head;
-  int node = total > 0 ? chunk(0, head) : -1;
-  float4 cm = make_float4(0.f, 0.f, 0.f, 0.f), ag = cm;
-  if (node >= 0) {
-    cm = __ldg(t.nd_cm + node);
-    ag = __ldg(t.nd_agg + node);
-  }
-  for (int base = 0; base < total; base += 32) {
-    int head_n = 0, node_n = -1;
-    float4 cm_n = make_float4(0.f, 0.f, 0.f, 0.f), ag_n = cm_n;
-    if (base + 32 < total) {
-      node_n = chunk(base + 32, head_n);
-      if (node_n >= 0) {
-        cm_n = __ldg(t.nd_cm + node_n);
-        ag_n = __ldg(t.nd_agg + node_n);
-      }
-    }
+    // Segment head: the last segment start at or before this lane (0: the
+    // segment runs on from the previous chunk).
+    const int head = max(31 - __clz(starts & upto), 0);
     V val = A::zero();
     int cnt = 0;
-    if (node >= 0) {
+    if (e < total) {
+      const int node = o_off + e;
       // Node record: an aggregate, or for a one-point leaf the point itself; a
       // negative diameter marks a leaf whose points must be summed.
+      const float4 cm = __ldg(t.nd_cm + node);
+      const float4 ag = __ldg(t.nd_agg + node);
       if (cm.w < 0.f) {
         const int4 tc = __ldg(t.nd_topo + node);
         val = add_leaf_points<A>(t, tc, q, kp, A::zero());
@@ -271,7 +252,7 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
         cnt = 1;
       }
     }
-    const bool counted = __any_sync(full, node >= 0 && cnt != 1);
+    const bool counted = __any_sync(full, e < total && cnt != 1);
     V x = val;
     int cx = cnt;
 #pragma unroll
@@ -294,10 +275,6 @@ __device__ __forceinline__ typename A::V expand(const DevTree& t, bool own, int 
       acc = A::add(acc, part);
       contribs += pc;
     }
-    node = node_n;
-    head = head_n;
-    cm = cm_n;
-    ag = ag_n;
   }
   return acc;
 }
