@@ -765,7 +765,7 @@ CAL_THETAS = (0.8, 0.6, 0.5, 0.4, 0.3, 0.25, 0.2, 0.15, 0.1, 0.07, 0.05)
 CAL_SCALES = (0.25, 0.5, 1.0, 2.0, 4.0, 8.0, 16.0)
 
 
-def serving_setup(C, seed=77, n_trees=32, n_requests=1500, device_trees=True):
+def serving_setup(C, seed=77, n_trees=32, n_requests=1500, device_trees=True, device=0):
     """32 resident trees (16 3D, 16 2D; Gaussian mixtures, torus, sphere and
     circle surfaces; 10^4..2*10^6 points log-uniform) and a seeded request list:
     tree, kernel (gravity / winding number / smooth distance alpha 100), query
@@ -792,8 +792,8 @@ def serving_setup(C, seed=77, n_trees=32, n_requests=1500, device_trees=True):
         t = dict(dim=dim, kind=kind, n=n, lo=lo, hi=hi, pts=pts, nrm=nrm, m=m)
         if device_trees:
             # built on the device (sbh_gpu_tree_build; the same trees as a host build)
-            t["bh"] = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=1)
-            t["sbh"] = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=2)
+            t["bh"] = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=1, device=device)
+            t["sbh"] = C.GpuTree.build(pts, nrm, m, lo, hi, dim_split_log=2, device=device)
             t["root2"] = t["sbh"].info.root_children
         trees.append(t)
     reqs = []
@@ -1002,11 +1002,72 @@ def serving_calibrate(C, W, torch, trees, reqs, refs):
     return out
 
 
+def run_serving_replicas(args, world, rank, local):
+    """Serving under torchrun: replicas only (the path has no exchange step).
+    Every rank holds its own copy of the 64 trees on its own GPU and serves the
+    same request stream; `value` is the device-resident batch and `e2e` the
+    server at saturation, each as all ranks' queries over the slowest rank's
+    time.  The plain path, the latency sweep and the CPU baseline are the
+    single-GPU line's."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import sbh_capi as C
+    import sbh_workloads as W
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    trees, reqs = serving_setup(C, device=local)
+    total_q = sum(r["nq"] for r in reqs)
+    entries, keep = device_batch(C, W, torch, trees, reqs, "served")
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    dist.barrier()
+    with ClockSampler(local) as clocks:
+        dev_ms = sum(timed_device(lambda: C.eval_batch(entries, stream=stream.cuda_stream),
+                                  stream, flush, args.warmup, args.steps))
+    del entries, keep
+    server = C.Server(device=local, slots=3, slot_queries=1 << 20, max_requests_per_batch=4096)
+    ids = {}
+    for i, t in enumerate(trees):
+        ids[(i, "sbh")] = server.add_tree(t["sbh"])
+        ids[(i, "bh")] = server.add_tree(t["bh"])
+    drive_served(C, W, trees, reqs[:50], server, ids, np.zeros(50))
+    dist.barrier()
+    served_s, _, _ = drive_served(C, W, trees, reqs, server, ids, np.zeros(len(reqs)))
+    server.close()
+    dev_ms, served_ms = max_over_ranks([dev_ms, served_s * 1e3], dist, dev)
+    dist.destroy_process_group()
+    if rank != 0:
+        return None
+    return {
+        "metric": METRIC, "value": whole_job_rate(world, total_q, dev_ms, args.steps),
+        "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generators; the reference publishes no dataset)",
+        "config": dict(serving_config(len(reqs), total_q), parallelism=f"replicas x{world}"),
+        "e2e": {"value": world * total_q / (served_ms / 1e3), "unit": "queries/s",
+                "h2d_bytes_per_step": world * sum(r["nq"] * 4 * trees[r["tree"]]["dim"]
+                                                  for r in reqs),
+                "d2h_bytes_per_step": world * total_q * 4, "ms_per_step": served_ms,
+                "path": "every rank's server (C ABI, host buffers), the stream submitted at "
+                        "t = 0; slowest rank"},
+        "clocks": clocks.summary(),
+        "gpu_launches": args.steps * 9,
+    }
+
+
 def run_serving(args):
     import torch
 
     import sbh_capi as C
     import sbh_workloads as W
+    world, rank, local = dist_setup()
+    if world > 1 and not args.calibrate:
+        return run_serving_replicas(args, world, rank, local)
     t_setup = time.perf_counter()
     trees, reqs = serving_setup(C)
     if args.calibrate:
@@ -1543,7 +1604,9 @@ def main():
     systems = {"serving": run_serving, "batching": run_batching,
                "differentiation": run_differentiation, "tree_build": run_tree_build}
     if args.workload in systems and args.impl == "ours":
-        print(json.dumps(systems[args.workload](args)), flush=True)
+        out = systems[args.workload](args)
+        if out is not None:
+            print(json.dumps(out), flush=True)
         return
     if args.workload == "serving":
         out = run_reference_serving(args)
