@@ -95,3 +95,21 @@ def test_device_pointer_entry_point(torus):
         ref, _, rcnt = gpu.eval(q, p, contribs=True)
         assert bits_equal(out.cpu().numpy(), ref)
         assert np.array_equal(cnt.cpu().numpy(), rcnt)
+
+
+@pytest.mark.parametrize("n", [1, 70000, 200003])
+def test_float64_queries_convert_exactly(torus, n):
+    """Queries passed as a C-ordered float64 (n, 3) array -- the reference's
+    callers' form -- are converted to float32 by the module's threads; the
+    results equal those of the same queries given as float32 bit for bit, for
+    every method."""
+    pts, nrm, a, lo, hi = torus
+    g1 = sbh_gpu.OctreeGPU1(sbh.Octree1(pts, nrm, a, lo, hi))
+    g2 = sbh_gpu.OctreeGPU2(sbh.Octree2(pts, nrm, a, lo, hi))
+    q64 = np.random.default_rng(n).uniform(-1.2, 1.2, (n, 3))
+    q32 = np.asfortranarray(q64.astype(np.float32))
+    assert q64.flags.c_contiguous
+    for f in (lambda q: sbh_gpu.eval_brute_force_gravity(g1, q),
+              lambda q: sbh_gpu.eval_barnes_hut_wn(g1, q, 2.0),
+              lambda q: sbh_gpu.multi_level_prefix_control_variate_gravity(g2, q, 1)):
+        assert bits_equal(f(q64)[0], f(q32)[0])
