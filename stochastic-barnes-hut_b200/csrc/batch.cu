@@ -189,7 +189,7 @@ __device__ __forceinline__ void run_bh(const DevTree& t, const BatchItem& it, lo
 }
 
 template <int DIM, int K>
-__device__ __forceinline__ void run_sbh(const DevTree& t, const BatchItem& it, long long u,
+__device__ __noinline__ void run_sbh(const DevTree& t, const BatchItem& it, long long u,
                                         const int* ord, float* scratch, int* status) {
   const SbhWarpSmem<float> ws = sbh_carve<float>(scratch);
   const long long s0 = u * it.unit_queries;
