@@ -255,6 +255,25 @@ def dist_setup():
     return world, rank, local
 
 
+def pair_pipe_bound(rates, kernel, dim=3):
+    """Pairs per second the all-pairs kernels' arithmetic allows: the slower of
+    the MUFU pipe (its measured rsqrt rate; every MUFU operation issues at that
+    rate) and the FP32 pipe (measured FFMA rate), for the operations a pair
+    costs in pairs.cuh: Plummer one rsqrt; gravity a sqrt and a reciprocal; the
+    winding number a reciprocal (and a sqrt in 3D); the smooth distance a sqrt,
+    and an exponential on the MUFU for three sources in four, on the FP32 pipe
+    (eight operations) for the fourth.  Returns (pairs/s, MUFU ops per pair,
+    FP32 lane operations per pair)."""
+    sub = 3 if dim == 3 else 2  # the differences; r^2 (or n.d) takes as many more
+    mufu, fp32 = {
+        "plummer": (1.0, 2 * sub + 1),
+        "gravity": (2.0, 2 * sub + 2),
+        "wn": (2.0 if dim == 3 else 1.0, 3 * sub + 4),
+        "smooth": (1.75, 2 * sub + 2 + 0.25 * 8),
+    }[kernel]
+    return min(rates["rsqrt_per_s"] / mufu, rates["ffma_per_s"] / fp32), mufu, fp32
+
+
 def dram_traffic(wl):
     """DRAM bytes per launch of the workload's main kernel (ncu), or None."""
     if wl.get("resized"):
@@ -414,18 +433,18 @@ def run_ours(args, wl):
     peak, peak_kind = load_peaks()
     traffic = dram_traffic(wl)
     if wl["method"] == "brute_force":
-        # Brute force is bound by the MUFU pipe: one rsqrt per Plummer pair (two
-        # MUFU ops -- rsqrt and reciprocal -- for gravity and the winding number).
+        # Brute force is bound by its arithmetic pipes (pair_pipe_bound).
         rates = C.measure_pipe_rates(local)
-        mufu_per_pair = 1 if wl["kernel"] == "plummer" else 2
+        bound, mufu_per_pair, fp32_per_pair = pair_pipe_bound(rates, wl["kernel"])
         pairs = float(nq) * float(wl["n"])
         roofline = {
             "bound": "sfu", "kernel": "brute_force_kernel",
-            "achieved": pairs / kmean_s, "peak": rates["rsqrt_per_s"] / mufu_per_pair,
-            "unit": "pairs/s", "frac": pairs / kmean_s / (rates["rsqrt_per_s"] / mufu_per_pair),
+            "achieved": pairs / kmean_s, "peak": bound,
+            "unit": "pairs/s", "frac": pairs / kmean_s / bound,
             "peak_source": "measured MUFU rsqrt rate (sbh_measure_pipe_rates): "
                            f"{rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
-                           f"{rates['sm_clock_mhz']:.0f} MHz; {mufu_per_pair} MUFU op(s) per pair",
+                           f"{rates['sm_clock_mhz']:.0f} MHz; {mufu_per_pair} MUFU op(s) and "
+                           f"{fp32_per_pair} FP32 lane op(s) per pair",
             "kernel_ms": statistics.mean(kern_ms), "pairs_per_launch": pairs,
             "pipe_rates": rates, "traffic": traffic,
         }
@@ -1217,9 +1236,8 @@ def serving_breakdown(C, W, torch, trees, reqs, stream, flush):
     """Each kernel's requests batched alone at their served operating points
     (device-resident, CUDA events): where the served batch's time goes, and the
     roofline of the largest part.  A part whose served point is brute force is
-    bound by the MUFU pipe (a reciprocal square root and an exponential or
-    reciprocal per pair): its pairs per second against the measured MUFU rate
-    halved; a traversal part is issue-bound and reported in queries/s."""
+    bound by its arithmetic pipes: its pairs per second against pair_pipe_bound;
+    a traversal part is issue-bound and reported in queries/s."""
     parts = {}
     for kern in SERVING_KERNELS:
         sub = [r for r in reqs if r["kernel"] == kern]
@@ -1234,12 +1252,14 @@ def serving_breakdown(C, W, torch, trees, reqs, stream, flush):
     p = parts[top]
     if p["op"][0] == "brute_force":
         rates = C.measure_pipe_rates(0)
-        peak = rates["rsqrt_per_s"] / 2.0
+        peak, mufu_per_pair, fp32_per_pair = pair_pipe_bound(rates, top)
         achieved = p["pairs"] / (p["ms"] / 1e3)
         roof = {"bound": "sfu", "kernel": "batch_eval_kernel (brute-force class), " + top,
                 "achieved": achieved, "peak": peak, "unit": "pairs/s", "frac": achieved / peak,
-                "peak_source": "measured MUFU rsqrt rate (sbh_measure_pipe_rates) / 2 MUFU "
-                               f"ops per pair: {rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
+                "peak_source": "measured MUFU rsqrt rate (sbh_measure_pipe_rates) / "
+                               f"{mufu_per_pair} MUFU ops per pair (3D operation counts; "
+                               f"{fp32_per_pair} FP32 lane ops against the measured FFMA rate "
+                               f"bind less): {rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
                                f"{rates['sm_clock_mhz']:.0f} MHz",
                 "kernel_ms": p["ms"], "pairs_per_launch": p["pairs"], "traffic": None,
                 "note": f"the {top} requests batched alone; share of the summed parts "

@@ -238,11 +238,13 @@ __device__ __forceinline__ void dispatch_unit(const DevTree& t, const BatchItem&
 
 // The persistent kernel of one method class: warps take that class's work
 // units from its counter and run them.  Minimum CTAs per SM: the single-call
-// kernels' occupancy (sampler 8 at 64 registers, Barnes-Hut 10 at 48).
+// kernels' occupancy (sampler 8 at 64 registers, Barnes-Hut 10 at 48); brute
+// force 4 (at most 128 registers; its unbounded 132 gave 3 CTAs per SM and
+// measured 6% slower).
 template <int CLASS>
 __global__ void __launch_bounds__(kEvalThreads, CLASS == kClassSbh  ? 8
                                                 : CLASS == kClassBh ? 10
-                                                                    : 1)
+                                                                    : 4)
     batch_eval_kernel(BatchHeader* hdr, const BatchItem* __restrict__ items,
                       const DevTree* __restrict__ trees, const int* __restrict__ order,
                       int* status, int warp_words, int stack_cap) {
@@ -435,7 +437,7 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
     it.unit_base = unit_base[batch_class(it.method)];
     // Work unit: sampler queries per warp (tuned); Barnes-Hut queries per warp
     // walk (tuned; vote keeps 32, its acceptance is defined over 32 queries);
-    // brute force 64 queries per warp (two per lane).
+    // brute force kBfUnitQueries per warp (query pairs per lane, tasks.cuh).
     it.unit_queries = it.method == 3   ? tuning.sampler_unit
                       : it.method == 1 ? tuning.bh_unit
                       : it.method == 0 ? kBfUnitQueries

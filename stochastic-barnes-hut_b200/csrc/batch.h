@@ -60,7 +60,7 @@ struct BatchHeader {
 };
 
 // Queries per work unit (one warp task) of warp-vote Barnes-Hut: 32, a lane
-// each (brute force takes kBfUnitQueries, two per lane).  The sampler's and
+// each (brute force takes kBfUnitQueries, 2 x kBfUnitPairs per lane).  The sampler's and
 // Barnes-Hut's unit sizes (queries per warp task) are tuned.
 constexpr int kUnitQueriesWarp = 32;
 

@@ -280,18 +280,32 @@ int enqueue_batch(BatchContext& ctx, const sbh_batch_item* items, int n_items,
   // which keeps its tree record in kernel parameters (the batch kernel reads
   // it from shared memory), on side streams forked here -- they read only the
   // caller's inputs -- so that they overlap the batch graph and each other.
+  // Longest first, each to the side stream with the least work queued so far
+  // (work ~ queries x sampled paths per query), so that the last kernels to
+  // start are short ones and the launches end together.
   if (!direct.empty()) {
     st = ensure_side_streams(ctx);
     if (st != SBH_OK) return st;
+    auto work = [](const sbh_batch_item* b) {
+      return (double)b->nq * ((double)b->params.samples_per_subdomain *
+                                  b->tree->dev.root_children + 1.0);
+    };
+    std::stable_sort(direct.begin(), direct.end(),
+                     [&](const sbh_batch_item* a, const sbh_batch_item* b) {
+                       return work(a) > work(b);
+                     });
     e = cudaEventRecord(ctx.fork, stream);
     for (int i = 0; i < BatchContext::kSide && e == cudaSuccess; i++)
       e = cudaStreamWaitEvent(ctx.side[i], ctx.fork, 0);
     if (e != cudaSuccess) return sbh::cuda_fail(e, "batch fork");  // nothing launched yet
+    double queued[BatchContext::kSide] = {};
     for (size_t k = 0; k < direct.size(); k++) {
       const sbh_batch_item* b = direct[k];
+      const int side = (int)(std::min_element(queued, queued + BatchContext::kSide) - queued);
+      queued[side] += work(b);
       st = sbh::enqueue_stochastic_direct(b->tree, b->params, b->d_queries, b->nq, b->d_results,
                                           b->d_contribs, b->d_self_mass, ctx.d_status,
-                                          ctx.side[k % BatchContext::kSide]);
+                                          ctx.side[side]);
       if (st != SBH_OK) break;
     }
   }

@@ -750,17 +750,20 @@ __device__ __forceinline__ void two_sum_add(float& hi, float& lo, float s) {
   lo += e;
 }
 
-// Queries per work unit of the batched brute-force task: two per lane.
-constexpr int kBfUnitQueries = 64;
+// Query pairs per lane of the batched brute-force task, and its queries per
+// work unit (a warp's 32 lanes x two queries per pair).  Two pairs per lane
+// (176 registers, fewer warps per SM) measured 15% slower than one on B200.
+constexpr int kBfUnitPairs = 1;
+constexpr int kBfUnitQueries = 64 * kBfUnitPairs;
 
-// Brute force for up to 64 queries at positions [slot0, slot_end) of a request,
-// one warp: the batch's brute-force task.  Lane l holds queries slot0 + l and
-// slot0 + 32 + l as one packed pair (the single-call kernel's FP32x2
-// arithmetic, pairs.cuh); the warp stages 32 sources at a time in its shared
-// memory (src / nrm, 32 entries each) with every coordinate duplicated into
-// both halves of a float2, and every lane reads them back as broadcasts.  Plain
-// FP32 sums over each 32 sources, merged into a (sum, error) pair per query by
-// two-sum.
+// Brute force for up to kBfUnitQueries queries at positions [slot0, slot_end)
+// of a request, one warp: the batch's brute-force task.  Lane l holds queries
+// slot0 + l + 32 j (j < 2 kBfUnitPairs) as packed pairs (j = 2p, 2p + 1): the
+// single-call kernel's FP32x2 arithmetic (pairs.cuh).  The warp stages 32
+// sources at a time in its shared memory (src / nrm, 32 entries each) with every
+// coordinate duplicated into both halves of a float2, and every lane reads them
+// back as broadcasts.  Plain FP32 sums over each 32 sources, merged into a
+// (sum, error) pair per query by two-sum.
 template <int DIM, int K>
 __device__ __forceinline__ void bf_warp_task(const DevTree& t, const float* __restrict__ qsoa,
                                              long long nq, long long slot0, long long slot_end,
@@ -769,15 +772,21 @@ __device__ __forceinline__ void bf_warp_task(const DevTree& t, const float* __re
                                              const float* __restrict__ self_mass, SrcPair* src,
                                              NrmPair* nrm) {
   constexpr bool kNormals = (K == kWindingNumber);
+  constexpr int NP = kBfUnitPairs;
   const int lane = threadIdx.x & 31;
-  const long long qa = slot0 + lane, qb = slot0 + 32 + lane;
-  float3 a = make_float3(0.f, 0.f, 0.f), b = a;
-  if (qa < slot_end) a = load_query<DIM>(qsoa, nq, qa);
-  if (qb < slot_end) b = load_query<DIM>(qsoa, nq, qb);
-  const float2 nqx = make_float2(-a.x, -b.x), nqy = make_float2(-a.y, -b.y),
-               nqz = make_float2(-a.z, -b.z);
-  float hia = 0.f, loa = 0.f, hib = 0.f, lob = 0.f;
-  const NrmPair no_normal = {};
+  float2 nqx[NP], nqy[NP], nqz[NP];
+  float hi[2 * NP], lo[2 * NP];
+#pragma unroll
+  for (int p = 0; p < NP; p++) {
+    const long long qa = slot0 + 64 * p + lane, qb = qa + 32;
+    float3 a = make_float3(0.f, 0.f, 0.f), b = a;
+    if (qa < slot_end) a = load_query<DIM>(qsoa, nq, qa);
+    if (qb < slot_end) b = load_query<DIM>(qsoa, nq, qb);
+    nqx[p] = make_float2(-a.x, -b.x);
+    nqy[p] = make_float2(-a.y, -b.y);
+    nqz[p] = make_float2(-a.z, -b.z);
+    hi[2 * p] = lo[2 * p] = hi[2 * p + 1] = lo[2 * p + 1] = 0.f;
+  }
   for (long long base = 0; base < t.n; base += 32) {
     const int len = (int)min(32LL, t.n - base);
     __syncwarp();  // every lane is done with the previous sources
@@ -790,32 +799,29 @@ __device__ __forceinline__ void bf_warp_task(const DevTree& t, const float* __re
       }
     }
     __syncwarp();
-    float2 part = make_float2(0.f, 0.f);
-    if (len == 32) {
-#pragma unroll 8
-      for (int k = 0; k < 32; k++)
-        part = accumulate2<DIM, K>(part, src[k], kNormals ? nrm[k] : no_normal, nqx, nqy, nqz, kp);
-    } else {
-      for (int k = 0; k < len; k++)
-        part = accumulate2<DIM, K>(part, src[k], kNormals ? nrm[k] : no_normal, nqx, nqy, nqz, kp);
+    float2 part[NP];
+#pragma unroll
+    for (int p = 0; p < NP; p++) part[p] = make_float2(0.f, 0.f);
+    if (len == 32)
+      accumulate_staged<DIM, K, NP, 32>(part, src, nrm, 32, nqx, nqy, nqz, kp);
+    else
+      accumulate_staged<DIM, K, NP, 0>(part, src, nrm, len, nqx, nqy, nqz, kp);
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+      two_sum_add(hi[2 * p], lo[2 * p], part[p].x);
+      two_sum_add(hi[2 * p + 1], lo[2 * p + 1], part[p].y);
     }
-    two_sum_add(hia, loa, part.x);
-    two_sum_add(hib, lob, part.y);
   }
-  float va = hia + loa, vb = hib + lob;
-  if (K == kGravity) {  // accumulate2 adds +m / (r + 0.1)
-    va = -va;
-    vb = -vb;
-  }
-  if (qa < slot_end) {
-    if (self_mass) va -= self_term<DIM, K>(a, __ldg(self_mass + qa), kp);
-    out[qa] = va;
-    if (contribs) contribs[qa] = (int)t.n;
-  }
-  if (qb < slot_end) {
-    if (self_mass) vb -= self_term<DIM, K>(b, __ldg(self_mass + qb), kp);
-    out[qb] = vb;
-    if (contribs) contribs[qb] = (int)t.n;
+#pragma unroll
+  for (int j = 0; j < 2 * NP; j++) {
+    const long long qi = slot0 + 32 * j + lane;
+    if (qi < slot_end) {
+      float v = hi[j] + lo[j];
+      if (K == kGravity) v = -v;  // accumulate2 adds +m / (r + 0.1)
+      if (self_mass) v -= self_term<DIM, K>(load_query<DIM>(qsoa, nq, qi), __ldg(self_mass + qi), kp);
+      out[qi] = v;
+      if (contribs) contribs[qi] = (int)t.n;
+    }
   }
 }
 

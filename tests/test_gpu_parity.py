@@ -72,6 +72,37 @@ def test_brute_force_matches_fp64(dim, kernel):
         assert np.abs(d_got - d_ref).max() <= 1e-6
 
 
+@pytest.mark.parametrize("batched", [False, True])
+def test_brute_force_smooth_distance_far_queries(batched):
+    # Every term is an FP32 subnormal (alpha * r between 90 and 103): the
+    # exponential's scaled form must keep them, in both the single-call kernel
+    # and the batched brute-force task.
+    pts, nrm, m = W.sphere_surface(20000, seed=31, radius=0.05)
+    lo, hi = W.padded_box(pts)
+    _, gpu = gpu_tree_from(pts, nrm, m, lo, hi)
+    rng = np.random.default_rng(32)
+    d = rng.normal(size=(3000, 3))
+    q = (d / np.linalg.norm(d, axis=1, keepdims=True) *
+         rng.uniform(0.95, 0.98, (3000, 1))).astype(np.float32)
+    alpha = 100.0
+    p = C.params(method=C.BRUTE_FORCE, kernel=C.SMOOTH_DIST, alpha=alpha)
+    if batched:
+        import torch
+        dq = torch.from_numpy(np.ascontiguousarray(q.T)).cuda()
+        out = torch.empty(len(q), dtype=torch.float32, device="cuda")
+        C.eval_batch([(gpu, p, dq.data_ptr(), len(q), out.data_ptr(), 0, 0)])
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+    else:
+        got, _ = gpu.eval(q, p)
+    ref = O.brute_force_f64(pts, nrm, m, C.SMOOTH_DIST, q, alpha=alpha)
+    nearest = np.sqrt(((q[:, None, :] - pts[None, ::7, :]) ** 2).sum(-1)).min()
+    assert alpha * nearest > 88.0  # exp(-88) < 2^-126: every term is subnormal
+    d_got = -np.log(got.astype(np.float64)) / alpha
+    d_ref = -np.log(ref) / alpha
+    assert np.abs(d_got - d_ref).max() <= 1e-6
+
+
 def test_brute_force_plain_small_workload():
     # Plummer potential over 65,536 Gaussian-mixture sources (the plain-method workload).
     pts, nrm, m = W.gaussian_mixture(65536, seed=21)
