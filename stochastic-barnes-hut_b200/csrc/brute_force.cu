@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(THREADS) brute_force_kernel(DevTree t,
   const long long chunk = (t.n + csize - 1) / csize;
   const long long c0 = min((long long)rank * chunk, t.n);
   const long long c1 = min(c0 + chunk, t.n);
+  const NrmPair no_normal = {};
   for (long long base = c0; base < c1; base += BF_TILE) {
     const int len = (int)min((long long)BF_TILE, c1 - base);
     for (int k = threadIdx.x; k < len; k += THREADS) {
@@ -89,12 +90,31 @@ __global__ void __launch_bounds__(THREADS) brute_force_kernel(DevTree t,
       float2 part[BF_PAIRS];
 #pragma unroll
       for (int p = 0; p < BF_PAIRS; p++) part[p] = make_float2(0.f, 0.f);
-      if (se - sb == BF_SUB)
-        accumulate_staged<DIM, K, BF_PAIRS, BF_SUB>(part, s_src + sb, s_nrm + (kNormals ? sb : 0),
-                                                    BF_SUB, nqx, nqy, nqz, kp);
-      else
-        accumulate_staged<DIM, K, BF_PAIRS, 0>(part, s_src + sb, s_nrm + (kNormals ? sb : 0),
-                                               se - sb, nqx, nqy, nqz, kp);
+      if (K == kSmoothDist) {
+        // its exponential split between the MUFU and the FP32 pipe (pairs.cuh)
+        const auto src = [&](int k) { return s_src[sb + k]; };
+        if (se - sb == BF_SUB)
+          accumulate_smooth<DIM, BF_PAIRS, BF_SUB>(part, src, BF_SUB, nqx, nqy, nqz, kp);
+        else
+          accumulate_smooth<DIM, BF_PAIRS, 0>(part, src, se - sb, nqx, nqy, nqz, kp);
+      } else if (se - sb == BF_SUB) {
+#pragma unroll 4
+        for (int k = sb; k < sb + BF_SUB; k++) {
+          const SrcPair sp = s_src[k];
+          const NrmPair np = kNormals ? s_nrm[k] : no_normal;
+#pragma unroll
+          for (int p = 0; p < BF_PAIRS; p++)
+            part[p] = accumulate2<DIM, K>(part[p], sp, np, nqx[p], nqy[p], nqz[p], kp);
+        }
+      } else {
+        for (int k = sb; k < se; k++) {
+          const SrcPair sp = s_src[k];
+          const NrmPair np = kNormals ? s_nrm[k] : no_normal;
+#pragma unroll
+          for (int p = 0; p < BF_PAIRS; p++)
+            part[p] = accumulate2<DIM, K>(part[p], sp, np, nqx[p], nqy[p], nqz[p], kp);
+        }
+      }
 #pragma unroll
       for (int p = 0; p < BF_PAIRS; p++) {
         two_sum_add(hi[2 * p], lo[2 * p], part[p].x);

@@ -156,26 +156,26 @@ __device__ __forceinline__ float2 accumulate2(float2 part, const SrcPair& s, con
   }
 }
 
-// part[p] += the kernel values of the staged sources src[0, n) (N > 0: n = N,
-// known at compile time) at query pair p.  The smooth distance with alpha >= 0
-// takes the scaled form (one source in kSdFmaEvery on the FP32 pipe) and
-// unscales the sums at the end; alpha < 0 (powers beyond the scaled range) and
-// every other kernel take the plain form.
-template <int DIM, int K, int NP, int N>
-__device__ __forceinline__ void accumulate_staged(float2 (&part)[NP], const SrcPair* src,
-                                                  const NrmPair* nrm, int n, const float2 (&nqx)[NP],
-                                                  const float2 (&nqy)[NP], const float2 (&nqz)[NP],
-                                                  const KParams& kp) {
-  constexpr bool kNormals = (K == kWindingNumber);
+// part[p] += the smooth-distance values of the staged sources 0 .. n-1 (N > 0:
+// n = N, known at compile time) at query pair p; src(k) returns staged source
+// k (an accessor, so that a caller indexing a __shared__ array keeps its
+// shared-memory loads).  alpha >= 0 takes the scaled form, one source in
+// kSdFmaEvery on the FP32 pipe, and unscales the sums at the end; alpha < 0
+// (powers beyond the scaled range) takes the plain form.
+template <int DIM, int NP, int N, class Src>
+__device__ __forceinline__ void accumulate_smooth(float2 (&part)[NP], const Src& src, int n,
+                                                  const float2 (&nqx)[NP], const float2 (&nqy)[NP],
+                                                  const float2 (&nqz)[NP], const KParams& kp) {
+  constexpr int K = kSmoothDist;
   const NrmPair none = {};
   const int count = N > 0 ? N : n;
-  if (K == kSmoothDist && kp.alpha >= 0.f) {
+  if (kp.alpha >= 0.f) {
     int k = 0;
 #pragma unroll 1
     for (; k + kSdFmaEvery <= count; k += kSdFmaEvery) {
 #pragma unroll
       for (int i = 0; i < kSdFmaEvery; i++) {
-        const SrcPair s = src[k + i];
+        const SrcPair s = src(k + i);
 #pragma unroll
         for (int p = 0; p < NP; p++)
           part[p] = i == 0 ? accumulate2<DIM, K, 2>(part[p], s, none, nqx[p], nqy[p], nqz[p], kp)
@@ -183,29 +183,19 @@ __device__ __forceinline__ void accumulate_staged(float2 (&part)[NP], const SrcP
       }
     }
     for (; k < count; k++) {
-      const SrcPair s = src[k];
+      const SrcPair s = src(k);
 #pragma unroll
       for (int p = 0; p < NP; p++)
         part[p] = accumulate2<DIM, K, 1>(part[p], s, none, nqx[p], nqy[p], nqz[p], kp);
     }
 #pragma unroll
     for (int p = 0; p < NP; p++) part[p] = __fmul2_rn(part[p], dup(kExp2Unscale));
-  } else if (N > 0) {
-#pragma unroll 4
-    for (int k = 0; k < N; k++) {
-      const SrcPair s = src[k];
-      const NrmPair nr = kNormals ? nrm[k] : none;
-#pragma unroll
-      for (int p = 0; p < NP; p++)
-        part[p] = accumulate2<DIM, K>(part[p], s, nr, nqx[p], nqy[p], nqz[p], kp);
-    }
   } else {
-    for (int k = 0; k < n; k++) {
-      const SrcPair s = src[k];
-      const NrmPair nr = kNormals ? nrm[k] : none;
+    for (int k = 0; k < count; k++) {
+      const SrcPair s = src(k);
 #pragma unroll
       for (int p = 0; p < NP; p++)
-        part[p] = accumulate2<DIM, K>(part[p], s, nr, nqx[p], nqy[p], nqz[p], kp);
+        part[p] = accumulate2<DIM, K>(part[p], s, none, nqx[p], nqy[p], nqz[p], kp);
     }
   }
 }

@@ -776,6 +776,7 @@ __device__ __forceinline__ void bf_warp_task(const DevTree& t, const float* __re
   const int lane = threadIdx.x & 31;
   float2 nqx[NP], nqy[NP], nqz[NP];
   float hi[2 * NP], lo[2 * NP];
+  const NrmPair no_normal = {};
 #pragma unroll
   for (int p = 0; p < NP; p++) {
     const long long qa = slot0 + 64 * p + lane, qb = qa + 32;
@@ -802,10 +803,29 @@ __device__ __forceinline__ void bf_warp_task(const DevTree& t, const float* __re
     float2 part[NP];
 #pragma unroll
     for (int p = 0; p < NP; p++) part[p] = make_float2(0.f, 0.f);
-    if (len == 32)
-      accumulate_staged<DIM, K, NP, 32>(part, src, nrm, 32, nqx, nqy, nqz, kp);
-    else
-      accumulate_staged<DIM, K, NP, 0>(part, src, nrm, len, nqx, nqy, nqz, kp);
+    if (K == kSmoothDist) {
+      // its exponential split between the MUFU and the FP32 pipe (pairs.cuh)
+      const auto srck = [&](int k) { return src[k]; };
+      if (len == 32)
+        accumulate_smooth<DIM, NP, 32>(part, srck, 32, nqx, nqy, nqz, kp);
+      else
+        accumulate_smooth<DIM, NP, 0>(part, srck, len, nqx, nqy, nqz, kp);
+    } else if (len == 32) {
+#pragma unroll 8
+      for (int k = 0; k < 32; k++) {
+        const NrmPair nr = kNormals ? nrm[k] : no_normal;
+#pragma unroll
+        for (int p = 0; p < NP; p++)
+          part[p] = accumulate2<DIM, K>(part[p], src[k], nr, nqx[p], nqy[p], nqz[p], kp);
+      }
+    } else {
+      for (int k = 0; k < len; k++) {
+        const NrmPair nr = kNormals ? nrm[k] : no_normal;
+#pragma unroll
+        for (int p = 0; p < NP; p++)
+          part[p] = accumulate2<DIM, K>(part[p], src[k], nr, nqx[p], nqy[p], nqz[p], kp);
+      }
+    }
 #pragma unroll
     for (int p = 0; p < NP; p++) {
       two_sum_add(hi[2 * p], lo[2 * p], part[p].x);
