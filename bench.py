@@ -1362,6 +1362,63 @@ def run_reference_serving(args):
     }
 
 
+# ------------------------------------------------- served smooth distance
+
+def run_served_smooth(args):
+    """The serving stream's smooth-distance requests (alpha 100) at their served
+    operating point, exact summation, as one device-resident batch: the largest
+    part of the served batch, where the batched brute-force class kernel runs
+    alone.  `--requests N` keeps the first N of them (a small case for
+    profiling); only the trees they name are built (host build + upload)."""
+    import torch
+
+    import sbh_capi as C
+    import sbh_workloads as W
+    trees, reqs = serving_setup(C, device_trees=False)
+    sub = [r for r in reqs if r["kernel"] == "smooth"]
+    if args.requests > 0:
+        sub = sub[:args.requests]
+    for ti in sorted({r["tree"] for r in sub}):
+        t = trees[ti]
+        t["bh"] = C.GpuTree(C.HostTree(t["pts"], t["nrm"], t["m"], t["lo"], t["hi"],
+                                       dim_split_log=1))
+    entries, keep = device_batch(C, W, torch, trees, sub, "served")
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    with ClockSampler(0) as clocks:
+        ms = timed_device(lambda: C.eval_batch(entries, stream=stream.cuda_stream), stream, flush,
+                          args.warmup, args.steps)
+    kms = statistics.mean(ms)
+    pairs = float(sum(r["nq"] * trees[r["tree"]]["n"] for r in sub))
+    pairs3 = float(sum(r["nq"] * trees[r["tree"]]["n"] for r in sub if trees[r["tree"]]["dim"] == 3))
+    rates = C.measure_pipe_rates(0)
+    peak = (pairs3 / pair_pipe_bound(rates, "smooth", 3)[0] +
+            (pairs - pairs3) / pair_pipe_bound(rates, "smooth", 2)[0])
+    peak = pairs / peak
+    achieved = pairs / (kms / 1e3)
+    nq = sum(r["nq"] for r in sub)
+    return {
+        "metric": "batched brute-force smooth-distance pairs/s (the serving stream's smooth "
+                  "requests, exact summation)",
+        "value": achieved, "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": kms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": f"served smooth distance: {len(sub)} requests of the serving "
+                               f"stream (alpha 100, {nq} queries, {pairs:.3e} pairs) as one "
+                               "sbh_eval_batch, queries resident, L2 flushed between steps"},
+        "queries_per_s": nq / (kms / 1e3),
+        "roofline": {"bound": "sfu", "kernel": "batch_eval_kernel (brute-force class)",
+                     "achieved": achieved, "peak": peak, "unit": "pairs/s",
+                     "frac": achieved / peak,
+                     "peak_source": "pair_pipe_bound per request dimension: measured MUFU rate "
+                                    f"{rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
+                                    f"{rates['sm_clock_mhz']:.0f} MHz, 1.75 MUFU ops per pair",
+                     "traffic": None},
+        "clocks": clocks.summary(),
+        "gpu_launches": args.steps * 9,
+    }
+
+
 # ---------------------------------------------------------------- batching
 
 def run_batching(args):
@@ -1602,7 +1659,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload",
                     choices=sorted(WORKLOADS) + ["serving", "batching", "differentiation",
-                                                 "tree_build"],
+                                                 "tree_build", "served_smooth"],
                     default="serving")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
@@ -1610,6 +1667,8 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=4096)
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
     ap.add_argument("--nq", type=int, default=0, help="override the query count (profiling)")
+    ap.add_argument("--requests", type=int, default=0,
+                    help="served_smooth: keep the first N smooth-distance requests (profiling)")
     ap.add_argument("--budget", type=int, default=0,
                     help="override the sampled paths per query of a stochastic workload")
     ap.add_argument("--stage-leaves", action="store_true",
@@ -1622,7 +1681,8 @@ def main():
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     systems = {"serving": run_serving, "batching": run_batching,
-               "differentiation": run_differentiation, "tree_build": run_tree_build}
+               "differentiation": run_differentiation, "tree_build": run_tree_build,
+               "served_smooth": run_served_smooth}
     if args.workload in systems and args.impl == "ours":
         out = systems[args.workload](args)
         if out is not None:

@@ -416,8 +416,23 @@ std::string BatchEngine::plan(std::vector<BatchItem>& items,
       tuning.bh_unit > 32)
     return "batch tuning out of range";
   if ((int)items.size() > lim_.max_items) return "too many requests in one batch";
-  std::stable_sort(items.begin(), items.end(), [](const BatchItem& a, const BatchItem& b) {
-    return batch_class(a.method) < batch_class(b.method);
+  for (const BatchItem& it : items)
+    if (it.tree < 0 || it.tree >= (int)host_trees.size()) return "request names an unknown tree";
+  // Grouped by class; within the brute-force and sampler classes, the requests
+  // whose work units cost most come first (brute force: sources per query;
+  // sampler: sampled paths per query), so that the class's warps take the long
+  // units early and the short ones fill in at the end.  The order changes no
+  // result: every unit is summed by one warp on its own.
+  auto unit_cost = [&](const BatchItem& it) -> double {
+    const DevTree& t = host_trees[it.tree];
+    if (batch_class(it.method) == kClassBf) return (double)t.n;
+    if (batch_class(it.method) == kClassSbh) return (double)it.samples * t.root_children;
+    return 0.0;
+  };
+  std::stable_sort(items.begin(), items.end(), [&](const BatchItem& a, const BatchItem& b) {
+    const int ca = batch_class(a.method), cb = batch_class(b.method);
+    if (ca != cb) return ca < cb;
+    return unit_cost(a) > unit_cost(b);
   });
   long long sort_base = 0, bucket_base = 0, unit_base[kClasses] = {0, 0, 0};
   for (BatchItem& it : items) {

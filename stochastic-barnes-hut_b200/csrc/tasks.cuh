@@ -499,8 +499,14 @@ __device__ __forceinline__ int sbh_round(const DevTree& t, float3 q, long long k
   V term = A::zero();
   int cnt = 0;
   while (__any_sync(0xffffffffu, own)) {
+    // Paths of this round that stand at the same node need its children sum
+    // once: the lowest such lane expands it and the others take its result.
+    const unsigned same = __match_any_sync(0xffffffffu, own ? prev : -1 - lane);
+    const int leader = __ffs(same) - 1;
     int cc;
-    const V sumc = expand<A>(t, own, prev, tprev, q, kp, lane, ws.ownlane(), cc);
+    V sumc = expand<A>(t, own && leader == lane, prev, tprev, q, kp, lane, ws.ownlane(), cc);
+    sumc = A::shfl(sumc, leader);
+    cc = __shfl_sync(0xffffffffu, cc, leader);
     if (own) {
       const float w = path_weight(t, prev, ws.path_spi()[lane], ev);
       const V kprev = A::node(__ldg(t.nd_cm + prev), __ldg(t.nd_agg + prev), q, kp);
