@@ -67,7 +67,8 @@ L2_FLUSH_BYTES = 512 << 20
 # figures are listed with the kernel's profile.  Null in the bench line when
 # the query count or budget is overridden.
 DRAM_TRAFFIC = {
-    "sbh_wn": 5.4615e9 + 0.2162e9,
+    "sbh_wn": 5.8709e9 + 0.2320e9,
+    "served_smooth": 194.35e6 + 7.80e6,
     "bh_wn": 307.58e6 + 31.53e6,
     "plain_small_bf": 1.85e6,
     "plain_small_bh": 3.36e6,
@@ -756,6 +757,11 @@ def run_reference(args, wl):
 # ----------------------------------------------------------------- serving
 
 SERVING_KERNELS = ("gravity", "wn", "smooth")
+# The server's slots: 3 batch contexts of up to 2^21 queries each.  Measured on
+# the stream submitted at t = 0 (two runs each): 3 x 2^20 queries 19.9-20.6 M
+# queries/s (p99 578-622 ms), 4 x 2^20 21.8-22.7 M, 2 x 2^22 22.2-24.9 M,
+# 3 x 2^21 23.9-24.2 M (p99 529-536 ms).
+SERVER_SLOT_QUERIES = 1 << 21
 SERVING_KID = {"gravity": 0, "wn": 1, "smooth": 2}  # SBH_KERNEL_* (the reference's KernelFuncID)
 SERVING_ALPHA = 100.0
 MATCH_TARGET = 1e-3
@@ -1048,7 +1054,8 @@ def run_serving_replicas(args, world, rank, local):
         dev_ms = sum(timed_device(lambda: C.eval_batch(entries, stream=stream.cuda_stream),
                                   stream, flush, args.warmup, args.steps))
     del entries, keep
-    server = C.Server(device=local, slots=3, slot_queries=1 << 20, max_requests_per_batch=4096)
+    server = C.Server(device=local, slots=3, slot_queries=SERVER_SLOT_QUERIES,
+                      max_requests_per_batch=4096)
     ids = {}
     for i, t in enumerate(trees):
         ids[(i, "sbh")] = server.add_tree(t["sbh"])
@@ -1139,7 +1146,8 @@ def run_serving(args):
         max(2, args.steps // 4)))
     del entries, keep
 
-    server = C.Server(slots=3, slot_queries=1 << 20, max_requests_per_batch=4096, tuning=tuning)
+    server = C.Server(slots=3, slot_queries=SERVER_SLOT_QUERIES, max_requests_per_batch=4096,
+                      tuning=tuning)
     ids = {}
     for i, t in enumerate(trees):
         ids[(i, "sbh")] = server.add_tree(t["sbh"])
@@ -1261,7 +1269,8 @@ def serving_breakdown(C, W, torch, trees, reqs, stream, flush):
                                f"{fp32_per_pair} FP32 lane ops against the measured FFMA rate "
                                f"bind less): {rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
                                f"{rates['sm_clock_mhz']:.0f} MHz",
-                "kernel_ms": p["ms"], "pairs_per_launch": p["pairs"], "traffic": None,
+                "kernel_ms": p["ms"], "pairs_per_launch": p["pairs"],
+                "traffic": DRAM_TRAFFIC.get("served_smooth") if top == "smooth" else None,
                 "note": f"the {top} requests batched alone; share of the summed parts "
                         f"{p['ms'] / sum(x['ms'] for x in parts.values()):.2f}"}
     else:
@@ -1413,7 +1422,7 @@ def run_served_smooth(args):
                      "peak_source": "pair_pipe_bound per request dimension: measured MUFU rate "
                                     f"{rates['rsqrt_per_clk_sm']:.2f}/clk/SM at "
                                     f"{rates['sm_clock_mhz']:.0f} MHz, 1.75 MUFU ops per pair",
-                     "traffic": None},
+                     "traffic": None if args.requests else DRAM_TRAFFIC.get("served_smooth")},
         "clocks": clocks.summary(),
         "gpu_launches": args.steps * 9,
     }
