@@ -1291,7 +1291,7 @@ def serving_config(n_requests, total_q):
                                      "stochastic_budget_factor": v["stochastic"]}
                                  for k, v in MATCHED.items()},
             "requests": n_requests, "queries": total_q,
-            "server": {"slots": 3, "slot_queries": 1 << 20},
+            "server": {"slots": 3, "slot_queries": SERVER_SLOT_QUERIES},
             "l2": "512 MiB buffer written between timed batch steps"}
 
 
