@@ -97,6 +97,35 @@ def test_batch_matches_single_calls(env):
             assert np.array_equal(cnt.cpu().numpy()[:len(q)], wcnt)
 
 
+def test_batch_results_do_not_depend_on_request_order(env):
+    # The engine reorders requests (by class, then by the cost of their work
+    # units); every unit is still summed by one warp on its own, so each
+    # request's results are the same bit for bit whatever order it was given in,
+    # brute force included.
+    torch, trees, gpus = env
+    rng = np.random.default_rng(95)
+    reqs = []
+    for name, method, kernel, nq, extra in REQUESTS:
+        if nq == 0:
+            continue
+        q = rng.uniform(-1.2, 1.2, (nq, gpus[name].dim)).astype(np.float32)
+        reqs.append((gpus[name], C.params(method=method, kernel=kernel, **extra), _dev(torch, q),
+                     nq))
+    stream = torch.cuda.current_stream().cuda_stream
+    results = []
+    for order in (list(range(len(reqs))), list(reversed(range(len(reqs)))),
+                  list(rng.permutation(len(reqs)))):
+        outs = [torch.empty(r[3], dtype=torch.float32, device="cuda") for r in reqs]
+        entries = [(reqs[i][0], reqs[i][1], reqs[i][2].data_ptr(), reqs[i][3],
+                    outs[i].data_ptr(), 0, 0) for i in order]
+        C.eval_batch(entries, stream=stream)
+        torch.cuda.synchronize()
+        results.append([o.cpu().numpy() for o in outs])
+    for other in results[1:]:
+        for a, b in zip(results[0], other):
+            assert bits_equal(a, b)
+
+
 def test_batch_excludes_self_terms(env):
     torch, trees, gpus = env
     pts, m = trees["gauss1_pts"]
