@@ -44,3 +44,17 @@ def test_serving_config_is_the_same_for_both_arms():
     a = B.serving_config(1500, 12799492)
     b = B.serving_config(1500, 12799492)
     assert a == b and a["operating_points"]["smooth"]["plain"] == ["brute_force", None]
+
+
+def test_pair_pipe_bound_counts():
+    # 16 MUFU operations and 128 FP32 lane operations per clock per SM: the
+    # all-pairs kernels are MUFU-bound, the smooth distance at 1.75 MUFU
+    # operations per pair (a sqrt; the exponential on the MUFU for three
+    # sources in four), the 2D winding number (one reciprocal) FP32-bound.
+    rates = {"rsqrt_per_s": 16.0, "ffma_per_s": 128.0}
+    for kernel, mufu in (("plummer", 1.0), ("gravity", 2.0), ("smooth", 1.75)):
+        bound, m, fp32 = B.pair_pipe_bound(rates, kernel, 3)
+        assert m == mufu and bound == 16.0 / mufu and 128.0 / fp32 > bound
+    bound, m, fp32 = B.pair_pipe_bound(rates, "wn", 2)
+    assert m == 1.0 and fp32 == 10 and bound == 12.8
+    assert B.pair_pipe_bound(rates, "smooth", 3)[2] == 10.0
