@@ -67,7 +67,7 @@ __device__ __forceinline__ float2 rcp2(float2 x) { return make_float2(mufu_rcp(x
 // smooth-distance pair costs two MUFU operations (the distance's sqrt and the
 // exponential) against about eight FP32 lane operations, and moving a quarter of
 // the exponentials to the FP32 pipe was the fastest split measured on B200
-// (one in two and one in three were slower).  Method: range reduction by
+// (one in two, three and five were slower).  Method: range reduction by
 // rounding, u = j + f, j = rint(u), f in [-1/2, 1/2] (j from the 1.5·2^23
 // rounding constant, whose low mantissa bits then hold j), a degree-5
 // polynomial for 2^f, and 2^j added to the exponent field as an integer.  The
